@@ -1,0 +1,63 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures)."""
+from __future__ import annotations
+
+import pytest
+import torch
+
+from conftest import golden_manifest, load_golden
+from oracle import ssn_oracle as O
+
+CASES = sorted(golden_manifest())
+
+
+def _rel(a, b):
+    return float(torch.linalg.vector_norm(a - b) / max(torch.linalg.vector_norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference(name, manifest):
+    meta = manifest[name]
+    data = load_golden(name)
+    T = torch.from_numpy(data["T"])
+    stats = O.DualStats()
+    if "error" in meta:
+        with pytest.raises(RuntimeError):
+            O.solve(T, stats)
+        return
+    X, omega, it = O.solve(T, stats)
+    assert it.tolist() == meta["iterations"]
+    assert stats.hvps == meta["counts"]["hvp_outer"]
+    assert stats.trials == meta["counts"]["line_change"]
+    assert _rel(X, torch.from_numpy(data["X"])) < 1e-10
+    assert _rel(omega, torch.from_numpy(data["omega"])) < 1e-10
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_inspect_output_matches_reference(name, manifest):
+    meta = manifest[name]
+    if "error" in meta:
+        pytest.skip("the reference raised on this input; no output to inspect")
+    data = load_golden(name)
+    T, X = torch.from_numpy(data["T"]), torch.from_numpy(data["X"])
+    recs = O.inspect_output(T, X)
+    ref = data["metrics"]
+    for rec, row in zip(recs, ref):
+        assert O.passes(rec)
+        for key, want in zip(("feasibility", "stationarity", "delta"), row):
+            # the metrics are residual-sized: compare on an absolute scale of the thresholds
+            assert abs(rec[key] - want) <= 1e-3 * O.THRESHOLDS[key] + 1e-6 * abs(want)
+
+
+def test_make_inputs_seed_rule():
+    T, seeds = O.make_inputs(8, 2, 1, 3)
+    assert seeds == [2026102100 + 1000 + j for j in range(3)]
+    g = torch.Generator().manual_seed(seeds[2])
+    want = torch.randn(16, 4, dtype=torch.float64, generator=g) / 4.0
+    assert torch.equal(T[2], want)
+
+
+def test_gram_fixture():
+    data = load_golden("n48_k12_b3")
+    Cr, Ci = O.gram(torch.from_numpy(data["T"]))
+    assert _rel(Cr, torch.from_numpy(data["Cr"])) < 1e-14
+    assert _rel(Ci, torch.from_numpy(data["Ci"])) < 1e-14
