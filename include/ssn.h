@@ -1,0 +1,172 @@
+/*
+ * ssn.h -- C ABI of the B200 (sm_100a) batched dual Newton-CG solver for the
+ * nearest real symplectic Stiefel matrix:
+ *
+ *     minimise ||X - T||_F^2   subject to   X^T J_2n X = J_2k,
+ *     J_2r = [[0, I_r], [-I_r, 0]],   T, X in R^{2n x 2k},  m = 2k.
+ *
+ * All arithmetic is IEEE FP64.  Every pointer argument is a DEVICE pointer to
+ * row-major, densely packed data unless stated otherwise; every call is
+ * asynchronous on the given stream (0 = legacy default stream) and returns an
+ * ssn_status.  No entry point allocates device memory: scratch comes from the
+ * caller-owned workspace (ssn_workspace_bytes), so the caller (PyTorch in the
+ * Python package) owns all memory, as in the reference where torch owns every
+ * tensor and kernels receive raw pointers (src/symplectic_projection/
+ * cuda_kernels.py:17-20).
+ *
+ * Limits: 1 <= k <= 64 (m <= 128), n >= k, batch >= 1.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the reference project root, yulinxie20/symplectic-stiefel-nearness).
+ */
+#ifndef SSN_H_
+#define SSN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* ssn_stream_t; /* == cudaStream_t */
+
+typedef enum {
+  SSN_OK = 0,
+  SSN_ERR_INVALID_ARGUMENT = 1, /* shape, pointer or option out of range      */
+  SSN_ERR_CUDA = 2,             /* a CUDA runtime call or launch failed          */
+  SSN_ERR_NEWTON_CAP = 3,       /* Newton cap reached (dual_recommended_hvp.py:191) */
+  SSN_ERR_LINE_SEARCH = 4,      /* no descent step in MAX_BACKTRACK halvings (:190) */
+  SSN_ERR_NONFINITE = 5,        /* NaN/Inf met in the input or the iteration      */
+  SSN_ERR_EIGH = 6,             /* Jacobi sweeps did not converge                  */
+  SSN_ERR_WORKSPACE = 7         /* workspace missing or too small                  */
+} ssn_status;
+
+/* Per-instance status words written by ssn_solve / ssn_dual (int32 per target). */
+enum {
+  SSN_INSTANCE_CONVERGED = 0,
+  SSN_INSTANCE_NEWTON_CAP = 3,
+  SSN_INSTANCE_LINE_SEARCH = 4,
+  SSN_INSTANCE_NONFINITE = 5,
+  SSN_INSTANCE_EIGH = 6
+};
+
+/* Solver constants; defaults follow dual_recommended_hvp.py:13-16. */
+typedef struct {
+  int max_newton;    /* 100 */
+  int max_cg;        /* 150 */
+  int max_backtrack; /* 40  */
+  double feas_tol;   /* 1e-8: an instance is done when residual < feas_tol / 2 */
+  int reserved[8];
+} ssn_options;
+
+/* Library version as 10000*major + 100*minor + patch. */
+int ssn_version(void);
+/* Static string naming a status code. */
+const char* ssn_status_string(int status);
+/* Fill *opt with the reference defaults. */
+void ssn_default_options(ssn_options* opt);
+
+/* Bytes of device workspace ssn_solve needs for this problem size. */
+size_t ssn_workspace_bytes(int batch, int n, int m);
+
+/*
+ * Full solve: T [batch, 2n, m] -> X [batch, 2n, m], omega [batch, m, m],
+ * iterations int64 [batch] (Newton updates per instance), status int32 [batch].
+ * Replaces symplectic_projection.solve (dual_recommended_hvp.py:231-242),
+ * i.e. gram_chunks (:79-96) + dual_batch (:99-191) + recover_matmul (:194-228),
+ * with device-resident input and output (no chunked PCIe staging).
+ * Returns SSN_OK when every instance converged, else the first failing
+ * instance's code (the reference raises RuntimeError for the whole batch).
+ */
+int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations,
+              int32_t* status, int batch, int n, int m,
+              void* workspace, size_t workspace_bytes,
+              const ssn_options* opt, ssn_stream_t stream);
+
+/*
+ * Gram products of T = [A; D]:  Cr = A^T A + D^T D,  Ci = A^T D - D^T A
+ * (overwritten, not accumulated).  A, D are [batch, rows, m] with batch
+ * strides ab_stride (elements, >= rows*m).  Replaces gram_add_
+ * (gram_triangle_reflect.py:19-36; kernels gram_offdiag / gram_diagonal,
+ * gram_triangle_reflect.cu:51-104).  Needs ssn_gram_workspace_bytes bytes.
+ */
+size_t ssn_gram_workspace_bytes(int batch, int rows, int m);
+int ssn_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
+             int batch, int rows, int m, void* workspace, size_t workspace_bytes,
+             ssn_stream_t stream);
+
+/*
+ * Recovery products:  Ur = A P^T + D Q^T,  Ui = D P^T - A Q^T.
+ * A, D, Ur, Ui are [batch, rows, m] with batch strides ab_stride / u_stride;
+ * P, Q are [batch, m, m] contiguous.  Replaces recover_block
+ * (recovery_fused.py:19-30; kernel recover_fused, recovery_fused.cu:2-41).
+ */
+int ssn_recover(const double* A, const double* D, int64_t ab_stride,
+                const double* P, const double* Q, double* Ur, double* Ui, int64_t u_stride,
+                int batch, int rows, int m, ssn_stream_t stream);
+
+/*
+ * Symmetric eigendecomposition of the scaled Gram matrix, Cr / s = V diag(w) V^T
+ * with s = max(1, trace(Cr)/m) (dual_recommended_hvp.py:106-108, where the
+ * reference calls torch.linalg.eigh).  Cyclic two-sided Jacobi in FP64;
+ * eigenvalues ascending.  scale may be NULL.  sweeps (may be NULL) receives
+ * the number of Jacobi sweeps per instance.
+ */
+int ssn_eigh(const double* Cr, double* values, double* vectors, double* scale,
+             int32_t* sweeps, int batch, int m, ssn_stream_t stream);
+
+/*
+ * Dual Newton-CG on given Gram matrices: (Cr, Ci) -> omega, and the final
+ * inverse parts P + iQ = (I + i omega)^-1, all in the original basis, plus
+ * iterations and status.  Replaces dual_batch (dual_recommended_hvp.py:99-191)
+ * with the `final` cache (:131-134).  Needs ssn_dual_workspace_bytes.
+ */
+size_t ssn_dual_workspace_bytes(int batch, int m);
+int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, double* Q,
+             int64_t* iterations, int32_t* status, int batch, int m,
+             void* workspace, size_t workspace_bytes, const ssn_options* opt,
+             ssn_stream_t stream);
+
+/* ---- component operations (mirrors of the reference kernel wrappers) ----
+ * All matrices [batch, m, m] contiguous FP64; vectors [batch] or [batch, m]. */
+
+/* U = E Sr, V = E Si.  Replaces inner_products (hvp_fused.py:22-34, hvp_inner, hvp_fused.cu:2-38). */
+int ssn_inner_products(const double* E, const double* Sr, const double* Si,
+                       double* U, double* V, int batch, int m, ssn_stream_t stream);
+/* H = Z - Z^T with Z = P U - Q V.  Replaces outer_skew (hvp_fused.py:37-53, hvp_outer*, hvp_fused.cu:83-238). */
+int ssn_outer_skew(const double* P, const double* Q, const double* U, const double* V,
+                   double* H, int batch, int m, ssn_stream_t stream);
+/* Yr = P diag(values) - Q Ci, Yi = P Ci + Q diag(values).
+ * Replaces sandwich_front (hvp_fused.py:56-69, hvp_sandwich_front, hvp_fused.cu:41-80). */
+int ssn_sandwich_front(const double* values, const double* Ci, const double* P, const double* Q,
+                       double* Yr, double* Yi, int batch, int m, ssn_stream_t stream);
+/* change[b] = <gradient, delta> + <V, delta_Sr + trial delta_Si>.
+ * Replaces line_change (hvp_fused.py:72-87, hvp_line_partial/finish, hvp_fused.cu:259-371). */
+int ssn_line_change(const double* gradient, const double* delta, const double* V,
+                    const double* delta_Sr, const double* trial, const double* delta_Si,
+                    double* change, int batch, int m, ssn_stream_t stream);
+/* out = 0.5 (R/den - (R/den)^T).  Replaces fused_precondition (hvp_fused.py:110-117, hvp_fused.cu:374-387). */
+int ssn_precondition(const double* R, const double* denominator, double* out,
+                     int batch, int m, ssn_stream_t stream);
+/* new_direction = direction + alpha p, new_r = r - alpha Hp (separately rounded).
+ * Replaces cg_update (hvp_fused.py:120-130, hvp_fused.cu:389-405). */
+int ssn_cg_update(const double* direction, const double* r, const double* p, const double* Hp,
+                  const double* alpha, double* new_direction, double* new_r,
+                  int batch, int m, ssn_stream_t stream);
+/* out = active ? z + beta p : 0.  Replaces cg_next (hvp_fused.py:133-143, hvp_fused.cu:407-420). */
+int ssn_cg_next(const double* z, const double* p, const double* beta, const uint8_t* active,
+                double* out, int batch, int m, ssn_stream_t stream);
+/* P = (L L^T)^-1 from a lower Cholesky factor, any m <= 128.  Replaces
+ * inverse_from_cholesky (cholesky_inverse_kernel.py:27-39, m = 128 only there). */
+int ssn_inverse_from_cholesky(const double* L, double* P, int batch, int m, ssn_stream_t stream);
+/* P = K^-1 for SPD K with a positive-definiteness flag (info[b] = 0 when every
+ * pivot is positive, else the 1-based failing pivot), the device equivalent of
+ * torch.linalg.cholesky_ex + construct_inverse (dual_recommended_hvp.py:173-176). */
+int ssn_spd_inverse(const double* K, double* P, int32_t* info, int batch, int m, ssn_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSN_H_ */

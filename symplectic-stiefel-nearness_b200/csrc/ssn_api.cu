@@ -1,0 +1,322 @@
+// ssn_api.cu -- the extern "C" entry points declared in include/ssn.h:
+// argument validation, workspace layout and the solve pipeline
+//   Gram (split-K + finalize) -> Jacobi eigh -> persistent dual Newton-CG -> recovery,
+// all enqueued on the caller's stream, with no host synchronisation.
+#include <stdint.h>
+#include <string.h>
+
+#include "ssn_common.cuh"
+#include "ssn_internal.h"
+
+namespace {
+
+using namespace ssn;
+
+constexpr int kVersion = 100;  // 0.1.0
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+bool shape_ok(int batch, int m) { return batch >= 1 && m >= 2 && m <= kMaxM && (m % 2) == 0; }
+
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? SSN_OK : SSN_ERR_CUDA; }
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Workspace layout of ssn_solve (byte offsets, 256-byte aligned sections).
+struct SolveLayout {
+  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, total;
+};
+
+SolveLayout solve_layout(int batch, int n, int m) {
+  const size_t mm = (size_t)m * m;
+  SolveLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off = align_up(off + bytes, 256);
+    return at;
+  };
+  L.cr = take(sizeof(double) * batch * mm);
+  L.ci = take(sizeof(double) * batch * mm);
+  L.values = take(sizeof(double) * batch * m);
+  L.vectors = take(sizeof(double) * batch * mm);
+  L.scale = take(sizeof(double) * batch);
+  L.pfin = take(sizeof(double) * batch * mm);
+  L.qfin = take(sizeof(double) * batch * mm);
+  // the Gram partial sums share the Newton workspace (they are dead before it is used)
+  const size_t work = sizeof(double) * (size_t)batch * kDualMats * mm;
+  const size_t partial = sizeof(double) * gram_partial_doubles(batch, n, m);
+  L.work = take(work > partial ? work : partial);
+  L.eig_status = take(sizeof(int32_t) * batch);
+  L.total = off;
+  return L;
+}
+
+struct DualLayout {
+  size_t values, vectors, scale, work, eig_status, total;
+};
+
+DualLayout dual_layout(int batch, int m) {
+  const size_t mm = (size_t)m * m;
+  DualLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off = align_up(off + bytes, 256);
+    return at;
+  };
+  L.values = take(sizeof(double) * batch * m);
+  L.vectors = take(sizeof(double) * batch * mm);
+  L.scale = take(sizeof(double) * batch);
+  L.work = take(sizeof(double) * (size_t)batch * kDualMats * mm);
+  L.eig_status = take(sizeof(int32_t) * batch);
+  L.total = off;
+  return L;
+}
+
+void fill_options(const ssn_options* opt, DualArgs& a) {
+  ssn_options d;
+  ssn_default_options(&d);
+  if (!opt) opt = &d;
+  a.max_newton = opt->max_newton;
+  a.max_cg = opt->max_cg;
+  a.max_backtrack = opt->max_backtrack;
+  a.feas_tol = opt->feas_tol;
+}
+
+bool options_ok(const ssn_options* opt) {
+  if (!opt) return true;
+  return opt->max_newton >= 1 && opt->max_newton <= 100000 && opt->max_cg >= 1 &&
+         opt->max_cg <= 100000 && opt->max_backtrack >= 1 && opt->max_backtrack <= 1074 &&
+         opt->feas_tol > 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ssn_version(void) { return kVersion; }
+
+const char* ssn_status_string(int status) {
+  switch (status) {
+    case SSN_OK: return "ok";
+    case SSN_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case SSN_ERR_CUDA: return "CUDA error";
+    case SSN_ERR_NEWTON_CAP: return "batched Newton iteration cap reached";
+    case SSN_ERR_LINE_SEARCH: return "batched line search found no descent step";
+    case SSN_ERR_NONFINITE: return "non-finite value in the iteration";
+    case SSN_ERR_EIGH: return "Jacobi eigensolver did not converge";
+    case SSN_ERR_WORKSPACE: return "workspace missing or too small";
+    default: return "unknown status";
+  }
+}
+
+void ssn_default_options(ssn_options* opt) {
+  if (!opt) return;
+  memset(opt, 0, sizeof(*opt));
+  opt->max_newton = 100;
+  opt->max_cg = 150;
+  opt->max_backtrack = 40;
+  opt->feas_tol = 1e-8;
+}
+
+size_t ssn_workspace_bytes(int batch, int n, int m) {
+  if (!shape_ok(batch, m) || n < m / 2) return 0;
+  return solve_layout(batch, n, m).total;
+}
+
+int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status,
+              int batch, int n, int m, void* workspace, size_t workspace_bytes,
+              const ssn_options* opt, ssn_stream_t stream_) {
+  if (!shape_ok(batch, m) || n < m / 2 || !T || !X || !omega || !iterations || !status ||
+      !options_ok(opt))
+    return SSN_ERR_INVALID_ARGUMENT;
+  if (!aligned16(T) || !aligned16(X) || !aligned16(omega)) return SSN_ERR_INVALID_ARGUMENT;
+  const SolveLayout L = solve_layout(batch, n, m);
+  if (!workspace || workspace_bytes < L.total || !aligned16(workspace)) return SSN_ERR_WORKSPACE;
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  char* ws = static_cast<char*>(workspace);
+  double* Cr = reinterpret_cast<double*>(ws + L.cr);
+  double* Ci = reinterpret_cast<double*>(ws + L.ci);
+  double* values = reinterpret_cast<double*>(ws + L.values);
+  double* vectors = reinterpret_cast<double*>(ws + L.vectors);
+  double* scale = reinterpret_cast<double*>(ws + L.scale);
+  double* Pf = reinterpret_cast<double*>(ws + L.pfin);
+  double* Qf = reinterpret_cast<double*>(ws + L.qfin);
+  double* work = reinterpret_cast<double*>(ws + L.work);
+  int32_t* eig_status = reinterpret_cast<int32_t*>(ws + L.eig_status);
+
+  const int64_t stride = 2LL * n * m;
+  const double* A = T;
+  const double* D = T + (size_t)n * m;
+  cudaError_t e = launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
+  if (e != cudaSuccess) return SSN_ERR_CUDA;
+  e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m, stream);
+  if (e != cudaSuccess) return SSN_ERR_CUDA;
+  DualArgs a{};
+  a.m = m;
+  fill_options(opt, a);
+  a.Cr = Cr;
+  a.Ci = Ci;
+  a.values = values;
+  a.vectors = vectors;
+  a.scale = scale;
+  a.eig_status = eig_status;
+  a.work = work;
+  a.omega = omega;
+  a.P = Pf;
+  a.Q = Qf;
+  a.iterations = iterations;
+  a.status = status;
+  a.counters = nullptr;
+  e = launch_dual(a, batch, stream);
+  if (e != cudaSuccess) return SSN_ERR_CUDA;
+  e = launch_recover(A, D, stride, Pf, Qf, X, X + (size_t)n * m, stride, batch, n, m, stream);
+  return cuda_status(e);
+}
+
+size_t ssn_gram_workspace_bytes(int batch, int rows, int m) {
+  if (!shape_ok(batch, m) || rows < 1) return 0;
+  return sizeof(double) * gram_partial_doubles(batch, rows, m);
+}
+
+int ssn_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci, int batch,
+             int rows, int m, void* workspace, size_t workspace_bytes, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || rows < 1 || !A || !D || !Cr || !Ci || ab_stride < (int64_t)rows * m ||
+      (ab_stride % 2) != 0 || !aligned16(A) || !aligned16(D))
+    return SSN_ERR_INVALID_ARGUMENT;
+  if (!workspace || workspace_bytes < ssn_gram_workspace_bytes(batch, rows, m) || !aligned16(workspace))
+    return SSN_ERR_WORKSPACE;
+  return cuda_status(launch_gram(A, D, ab_stride, Cr, Ci, batch, rows, m,
+                                 static_cast<double*>(workspace),
+                                 reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_recover(const double* A, const double* D, int64_t ab_stride, const double* P, const double* Q,
+                double* Ur, double* Ui, int64_t u_stride, int batch, int rows, int m,
+                ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || rows < 1 || !A || !D || !P || !Q || !Ur || !Ui ||
+      ab_stride < (int64_t)rows * m || u_stride < (int64_t)rows * m || (ab_stride % 2) != 0 ||
+      (u_stride % 2) != 0 || !aligned16(A) || !aligned16(D) || !aligned16(P) || !aligned16(Q))
+    return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_recover(A, D, ab_stride, P, Q, Ur, Ui, u_stride, batch, rows, m,
+                                    reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_eigh(const double* Cr, double* values, double* vectors, double* scale, int32_t* sweeps,
+             int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !Cr || !values || !vectors) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_eigh(Cr, values, vectors, scale, sweeps, nullptr, batch, m,
+                                 reinterpret_cast<cudaStream_t>(stream)));
+}
+
+size_t ssn_dual_workspace_bytes(int batch, int m) {
+  if (!shape_ok(batch, m)) return 0;
+  return dual_layout(batch, m).total;
+}
+
+int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, double* Q,
+             int64_t* iterations, int32_t* status, int batch, int m, void* workspace,
+             size_t workspace_bytes, const ssn_options* opt, ssn_stream_t stream_) {
+  if (!shape_ok(batch, m) || !Cr || !Ci || !omega || !P || !Q || !iterations || !status ||
+      !options_ok(opt) || !aligned16(Cr) || !aligned16(Ci))
+    return SSN_ERR_INVALID_ARGUMENT;
+  const DualLayout L = dual_layout(batch, m);
+  if (!workspace || workspace_bytes < L.total || !aligned16(workspace)) return SSN_ERR_WORKSPACE;
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  char* ws = static_cast<char*>(workspace);
+  double* values = reinterpret_cast<double*>(ws + L.values);
+  double* vectors = reinterpret_cast<double*>(ws + L.vectors);
+  double* scale = reinterpret_cast<double*>(ws + L.scale);
+  int32_t* eig_status = reinterpret_cast<int32_t*>(ws + L.eig_status);
+  cudaError_t e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m, stream);
+  if (e != cudaSuccess) return SSN_ERR_CUDA;
+  DualArgs a{};
+  a.m = m;
+  fill_options(opt, a);
+  a.Cr = Cr;
+  a.Ci = Ci;
+  a.values = values;
+  a.vectors = vectors;
+  a.scale = scale;
+  a.eig_status = eig_status;
+  a.work = reinterpret_cast<double*>(ws + L.work);
+  a.omega = omega;
+  a.P = P;
+  a.Q = Q;
+  a.iterations = iterations;
+  a.status = status;
+  a.counters = nullptr;
+  return cuda_status(launch_dual(a, batch, stream));
+}
+
+#define SSN_CHECK_MATS(...)                                                   \
+  do {                                                                        \
+    const void* ps_[] = {__VA_ARGS__};                                        \
+    for (const void* p_ : ps_)                                                \
+      if (!p_ || !aligned16(p_)) return SSN_ERR_INVALID_ARGUMENT;             \
+  } while (0)
+
+int ssn_inner_products(const double* E, const double* Sr, const double* Si, double* U, double* V,
+                       int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m)) return SSN_ERR_INVALID_ARGUMENT;
+  SSN_CHECK_MATS(E, Sr, Si, U, V);
+  return cuda_status(launch_inner_products(E, Sr, Si, U, V, batch, m, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_outer_skew(const double* P, const double* Q, const double* U, const double* V, double* H,
+                   int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m)) return SSN_ERR_INVALID_ARGUMENT;
+  SSN_CHECK_MATS(P, Q, U, V, H);
+  return cuda_status(launch_outer_skew(P, Q, U, V, H, batch, m, nullptr, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_sandwich_front(const double* values, const double* Ci, const double* P, const double* Q,
+                       double* Yr, double* Yi, int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !values) return SSN_ERR_INVALID_ARGUMENT;
+  SSN_CHECK_MATS(Ci, P, Q, Yr, Yi);
+  return cuda_status(launch_sandwich_front(values, Ci, P, Q, Yr, Yi, batch, m,
+                                           reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_line_change(const double* gradient, const double* delta, const double* V,
+                    const double* delta_Sr, const double* trial, const double* delta_Si,
+                    double* change, int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !change) return SSN_ERR_INVALID_ARGUMENT;
+  SSN_CHECK_MATS(gradient, delta, V, delta_Sr, trial, delta_Si);
+  return cuda_status(launch_line_change(gradient, delta, V, delta_Sr, trial, delta_Si, change, batch, m,
+                                        reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_precondition(const double* R, const double* denominator, double* out, int batch, int m,
+                     ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !R || !denominator || !out) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_precondition(R, denominator, out, batch, m, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_cg_update(const double* direction, const double* r, const double* p, const double* Hp,
+                  const double* alpha, double* new_direction, double* new_r, int batch, int m,
+                  ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !direction || !r || !p || !Hp || !alpha || !new_direction || !new_r)
+    return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_cg_update(direction, r, p, Hp, alpha, new_direction, new_r, batch, m,
+                                      reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_cg_next(const double* z, const double* p, const double* beta, const uint8_t* active,
+                double* out, int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !z || !p || !beta || !active || !out) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_cg_next(z, p, beta, active, out, batch, m, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_inverse_from_cholesky(const double* L, double* P, int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !L || !P) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_inverse_from_cholesky(L, P, batch, m, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_spd_inverse(const double* K, double* P, int32_t* info, int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !K || !P || !info) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_spd_inverse(K, P, info, batch, m, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+}  // extern "C"

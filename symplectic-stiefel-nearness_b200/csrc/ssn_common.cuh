@@ -1,0 +1,295 @@
+// ssn_common.cuh -- shared device helpers for the sm_100a symplectic Stiefel solver.
+//
+// * FP64 tensor-core fragments: mma.sync m8n8k4 f64 (DMMA).  On B200 it runs at
+//   the same 37 TFLOP/s as SIMT DFMA but issues 256 FMAs per warp instruction and
+//   reuses register fragments, so products reach the FP64 pipe limit with far
+//   fewer issue slots and shared-memory reads.  tcgen05 has no f64 kind.
+// * cp.async 16-byte global->shared copies for K-panel double buffering.
+// * Deterministic CTA reductions: fixed shuffle tree + fixed-order warp sum, so
+//   every thread of a CTA sees bit-identical scalars and takes the same branch.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ssn.h"
+
+namespace ssn {
+
+constexpr int kMaxM = 128;      // m = 2k <= 128
+constexpr int kThreads = 512;   // CTA size of the Newton / component kernels
+constexpr int kWarps = kThreads / 32;
+constexpr int kPanelK = 16;     // K extent of one staged panel
+constexpr int kMinorLd = 20;    // leading dim of K-minor panels (== 4 mod 16)
+
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+__host__ __device__ constexpr int round_up(int a, int b) { return cdiv(a, b) * b; }
+// Smallest leading dimension >= x with ld == 4 (mod 16) doubles: DMMA fragment
+// loads (8 rows x 4 k, or 4 k x 8 cols) then hit 16 distinct bank pairs per half-warp.
+__host__ __device__ constexpr int frag_ld(int x) { return x + (((4 - x) % 16) + 16) % 16; }
+__host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
+
+// m-bucket: products are tiled for mp <= 32*MB.
+__host__ __device__ constexpr int bucket_of(int m) { return m <= 32 ? 1 : m <= 64 ? 2 : m <= 96 ? 3 : 4; }
+
+// ---------------------------------------------------------------- PTX wrappers
+// D = A(8x4, row) * B(4x8, col) + C.  Lane l: g = l>>2, t = l&3;
+// a = A[g][t], b = B[t][g], {c0,c1} = C[g][2t], C[g][2t+1].
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(c0), "+d"(c1)
+      : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async_16(void* smem_dst, const void* gmem_src) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the CTA; every thread returns the same bits.  red: >= kWarps doubles.
+template <int THREADS = kThreads>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < THREADS / 32; ++w) s += red[w];
+  return s;
+}
+
+// Two sums with one pair of barriers.  red: >= 2*kWarps doubles.
+template <int THREADS = kThreads>
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* red) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = a;
+    red[THREADS / 32 + (threadIdx.x >> 5)] = b;
+  }
+  __syncthreads();
+  double sa = 0.0, sb = 0.0;
+#pragma unroll
+  for (int w = 0; w < THREADS / 32; ++w) {
+    sa += red[w];
+    sb += red[THREADS / 32 + w];
+  }
+  a = sa;
+  b = sb;
+}
+
+// ---------------------------------------------------------------- product engine
+// One operand of a product: op = stored or stored^T, stored row-major with
+// leading dimension ld.  alias >= 0 (B operands only): reuse the smem panel of
+// A operand `alias` (same stored data and the same K-major layout); valid only
+// when that A operand is transposed and the product runs in one row pass with
+// R == N, so the A panel covers exactly the B columns.
+struct MatOp {
+  const double* ptr;
+  int ld;
+  int trans;
+  int alias;
+};
+
+__device__ __forceinline__ MatOp op_n(const double* p, int ld) { return MatOp{p, ld, 0, -1}; }
+__device__ __forceinline__ MatOp op_t(const double* p, int ld) { return MatOp{p, ld, 1, -1}; }
+
+// Coefficient table: 2 bits per (out, a, b): 1 = +, 2 = -.  Index (o*4 + a*2 + b).
+__host__ __device__ constexpr uint32_t coef_bit(int o, int a, int b, int s) {
+  return static_cast<uint32_t>(s) << (2 * (o * 4 + a * 2 + b));
+}
+__host__ __device__ constexpr int coef_get(uint32_t c, int o, int a, int b) {
+  return static_cast<int>((c >> (2 * (o * 4 + a * 2 + b))) & 3u);
+}
+
+// Copy one K-panel [k0, k0+16) of an operand into a shared slot, zero-filling
+// outside [0,outer) x [0,K) up to the padded extent.
+//   kminor: slot[o * kMinorLd + kk] = stored[o][k0+kk]   (o < outer_pad)
+//   kmajor: slot[kk * pld + o]      = stored[k0+kk][o]
+__device__ __forceinline__ void load_panel(double* slot, const double* ptr, int ld, bool kminor,
+                                           int outer, int outer_pad, int pld, int k0, int K) {
+  if (kminor) {
+    const int chunks = outer_pad * (kPanelK / 2);
+    for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+      const int o = c >> 3, kk = (c & 7) * 2, k = k0 + kk;
+      double* dst = slot + o * kMinorLd + kk;
+      if (o < outer && k + 1 < K) {
+        cp_async_16(dst, ptr + (size_t)o * ld + k);
+      } else {
+        dst[0] = (o < outer && k < K) ? ptr[(size_t)o * ld + k] : 0.0;
+        dst[1] = 0.0;
+      }
+    }
+  } else {
+    const int half = outer_pad / 2;
+    const int chunks = kPanelK * half;
+    for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+      const int kk = c / half, o = (c - kk * half) * 2, k = k0 + kk;
+      double* dst = slot + kk * pld + o;
+      if (k < K && o + 1 < outer) {
+        cp_async_16(dst, ptr + (size_t)k * ld + o);
+      } else {
+        dst[0] = (k < K && o < outer) ? ptr[(size_t)k * ld + o] : 0.0;
+        dst[1] = 0.0;
+      }
+    }
+  }
+}
+
+// CTA-wide product engine (kThreads threads, warps on a 4x4 grid).
+//   out_o[r][c] = sum_{a,b} sign(o,a,b) * op(A_a)[r][:] . op(B_b)[:][c]
+// for r < R, c < N, contraction K, with R, N <= 128.  Each warp owns a
+// (WR*8) x (WC*8) tile; row passes of 4*WR*8 rows cover R.  Results are handed
+// to epi(o, r, c, value) for every valid (r, c).  smem: 2 stages x 4 slots of
+// `slot` doubles.  All threads must call it; it ends with __syncthreads().
+template <int WR, int WC, int NA, int NB, int NOUT, uint32_t COEF, class Epi>
+__device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (&B)[NB], int R, int N, int K,
+                                   double* smem, int slot, Epi& epi) {
+  static_assert(NA >= 1 && NA <= 2 && NB >= 1 && NB <= 2 && NOUT >= 1 && NOUT <= 2, "engine arity");
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wrow = warp >> 2, wcol = warp & 3;
+  constexpr int RP = 4 * WR * 8;
+  const int npanel = cdiv(K, kPanelK);
+  const int N_pad = round_up(N, 8);
+  const int pldB = frag_ld(N_pad);
+
+  for (int r0 = 0; r0 < R; r0 += RP) {
+    const int Rp = imin(RP, R - r0);
+    const int Rp_pad = round_up(Rp, 8);
+    const int pldA = frag_ld(Rp_pad);
+    double acc[NOUT][WR][WC][2];
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+      for (int i = 0; i < WR; ++i)
+#pragma unroll
+        for (int j = 0; j < WC; ++j) acc[o][i][j][0] = acc[o][i][j][1] = 0.0;
+
+    auto issue = [&](int stage, int k0) {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        const bool kminor = !A[a].trans;
+        const double* base = A[a].trans ? A[a].ptr + r0 : A[a].ptr + (size_t)r0 * A[a].ld;
+        load_panel(smem + (stage * 4 + a) * slot, base, A[a].ld, kminor, Rp, Rp_pad, pldA, k0, K);
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        if (B[b].alias >= 0) continue;
+        const bool kminor = B[b].trans;
+        load_panel(smem + (stage * 4 + 2 + b) * slot, B[b].ptr, B[b].ld, kminor, N, N_pad, pldB, k0, K);
+      }
+      cp_async_commit();
+    };
+
+    const int row_base = wrow * WR * 8;
+    const int col_base = wcol * WC * 8;
+    issue(0, 0);
+    for (int kp = 0; kp < npanel; ++kp) {
+      if (kp + 1 < npanel) {
+        issue((kp + 1) & 1, (kp + 1) * kPanelK);
+      } else {
+        cp_async_commit();
+      }
+      cp_async_wait<1>();
+      __syncthreads();
+      const int stage = kp & 1;
+      if (row_base < Rp && col_base < N) {
+#pragma unroll
+        for (int ks = 0; ks < kPanelK / 4; ++ks) {
+          const int kk = ks * 4 + t;
+          double af[NA][WR], bf[NB][WC];
+#pragma unroll
+          for (int a = 0; a < NA; ++a) {
+            const double* s = smem + (stage * 4 + a) * slot;
+#pragma unroll
+            for (int i = 0; i < WR; ++i) {
+              // sub-tiles past the padded row extent are never read (they may lie past the slot)
+              const int r = row_base + i * 8 + g;
+              af[a][i] = (row_base + i * 8 < Rp) ? (A[a].trans ? s[kk * pldA + r] : s[r * kMinorLd + kk]) : 0.0;
+            }
+          }
+#pragma unroll
+          for (int b = 0; b < NB; ++b) {
+            const int sl = B[b].alias >= 0 ? B[b].alias : 2 + b;
+            const double* s = smem + (stage * 4 + sl) * slot;
+            const int ld = B[b].alias >= 0 ? pldA : pldB;
+            const bool kminor = B[b].alias >= 0 ? false : (B[b].trans != 0);
+#pragma unroll
+            for (int j = 0; j < WC; ++j) {
+              const int c = col_base + j * 8 + g;
+              bf[b][j] = (col_base + j * 8 < N) ? (kminor ? s[c * kMinorLd + kk] : s[kk * ld + c]) : 0.0;
+            }
+          }
+#pragma unroll
+          for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+            for (int a = 0; a < NA; ++a)
+#pragma unroll
+              for (int b = 0; b < NB; ++b) {
+                const int sg = coef_get(COEF, o, a, b);
+                if (sg == 0) continue;
+#pragma unroll
+                for (int i = 0; i < WR; ++i) {
+                  if (row_base + i * 8 >= Rp) continue;
+                  const double av = sg == 2 ? -af[a][i] : af[a][i];
+#pragma unroll
+                  for (int j = 0; j < WC; ++j) {
+                    if (col_base + j * 8 >= N) continue;
+                    dmma_8x8x4(acc[o][i][j][0], acc[o][i][j][1], av, bf[b][j]);
+                  }
+                }
+              }
+        }
+      }
+      __syncthreads();
+    }
+    cp_async_wait<0>();
+    // epilogue
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+      for (int i = 0; i < WR; ++i)
+#pragma unroll
+        for (int j = 0; j < WC; ++j)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int r = row_base + i * 8 + g;
+            const int c = col_base + j * 8 + 2 * t + e;
+            if (r < Rp && c < N) epi(o, r0 + r, c, acc[o][i][j][e]);
+          }
+    __syncthreads();
+  }
+}
+
+// Warp-tile shape for bucket MB (mp <= 32*MB) and NOUT accumulator sets,
+// keeping NOUT*WR*WC*2 <= 36 doubles of accumulators per thread.
+template <int MB, int NOUT>
+struct Tile {
+  static constexpr int WC = MB;
+  static constexpr int WR = imin(MB == 1 ? 4 : MB, imax(1, 18 / (NOUT * WC)));
+  static constexpr int ROWS = 4 * WR * 8;  // rows per pass
+};
+
+// Shared-memory slot size (doubles) for bucket MB.
+__host__ __device__ constexpr int slot_doubles(int MB) {
+  return imax(32 * MB * kMinorLd, kPanelK * frag_ld(32 * MB));
+}
+__host__ __device__ constexpr int slot_doubles_rows(int rows, int MB) {
+  return imax(imax(rows, 32 * MB) * kMinorLd, kPanelK * frag_ld(imax(rows, 32 * MB)));
+}
+
+}  // namespace ssn

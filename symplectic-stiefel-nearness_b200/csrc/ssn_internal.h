@@ -1,0 +1,70 @@
+// ssn_internal.h -- host-side launch helpers shared by the translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "ssn.h"
+
+namespace ssn {
+
+// Number of m x m FP64 matrices of per-instance dual workspace.
+constexpr int kDualMats = 21;
+
+struct DualArgs {
+  int m;
+  int max_newton, max_cg, max_backtrack;
+  double feas_tol;
+  const double* Cr;        // [B,m,m] (unscaled)
+  const double* Ci;        // [B,m,m]
+  const double* values;    // [B,m]   eigenvalues of Cr/s
+  const double* vectors;   // [B,m,m] eigenvectors
+  const double* scale;     // [B]
+  const int32_t* eig_status;  // [B]
+  double* work;            // [B, kDualMats, m, m]
+  double* omega;           // [B,m,m] out, original basis
+  double* P;               // [B,m,m] out
+  double* Q;               // [B,m,m] out
+  int64_t* iterations;     // [B] out
+  int32_t* status;         // [B] out
+  int32_t* counters;       // [B,4] out: newton steps, hvps, trials, fallbacks (may be null)
+};
+
+size_t eigh_smem_bytes(int m);
+cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, double* scale,
+                        int32_t* sweeps, int32_t* status, int batch, int m, cudaStream_t stream);
+cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
+
+size_t gram_partial_doubles(int batch, int rows, int m);
+cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
+                        int batch, int rows, int m, double* partial, cudaStream_t stream);
+cudaError_t launch_recover(const double* A, const double* D, int64_t ab_stride, const double* P,
+                           const double* Q, double* Ur, double* Ui, int64_t u_stride, int batch,
+                           int rows, int m, cudaStream_t stream);
+
+// component kernels (mirrors of the reference wrappers)
+cudaError_t launch_inner_products(const double* E, const double* Sr, const double* Si, double* U,
+                                  double* V, int batch, int m, cudaStream_t stream);
+cudaError_t launch_outer_skew(const double* P, const double* Q, const double* U, const double* V,
+                              double* H, int batch, int m, double* scratch, cudaStream_t stream);
+cudaError_t launch_sandwich_front(const double* values, const double* Ci, const double* P,
+                                  const double* Q, double* Yr, double* Yi, int batch, int m,
+                                  cudaStream_t stream);
+cudaError_t launch_line_change(const double* g, const double* delta, const double* V,
+                               const double* dSr, const double* trial, const double* dSi,
+                               double* change, int batch, int m, cudaStream_t stream);
+cudaError_t launch_precondition(const double* R, const double* den, double* out, int batch, int m,
+                                cudaStream_t stream);
+cudaError_t launch_cg_update(const double* d, const double* r, const double* p, const double* Hp,
+                             const double* alpha, double* nd, double* nr, int batch, int m,
+                             cudaStream_t stream);
+cudaError_t launch_cg_next(const double* z, const double* p, const double* beta,
+                           const uint8_t* active, double* out, int batch, int m,
+                           cudaStream_t stream);
+cudaError_t launch_spd_inverse(const double* K, double* P, int32_t* info, int batch, int m,
+                               cudaStream_t stream);
+cudaError_t launch_inverse_from_cholesky(const double* L, double* P, int batch, int m,
+                                         cudaStream_t stream);
+
+}  // namespace ssn

@@ -1,0 +1,104 @@
+"""ctypes binding of the C ABI in ``include/ssn.h`` (``libssn.so``).
+
+This is the only route from Python to the compute path: there is no CPU or
+library fallback.  Loading fails loudly when the library is missing, and every
+compute call requires CUDA float64 tensors on one device.  Arguments are raw
+device pointers and sizes; kernels run on torch's current CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "libssn.so"
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_SZ = ctypes.c_size_t
+
+# name: (restype, argtypes) -- mirrors include/ssn.h
+PROTOTYPES = {
+    "ssn_version": (_I, []),
+    "ssn_status_string": (ctypes.c_char_p, [_I]),
+    "ssn_default_options": (None, [_P]),
+    "ssn_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "ssn_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
+    "ssn_gram_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P]),
+    "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P]),
+    "ssn_eigh": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_dual_workspace_bytes": (_SZ, [_I, _I]),
+    "ssn_dual": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
+    "ssn_inner_products": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_outer_skew": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_sandwich_front": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_line_change": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_precondition": (_I, [_P, _P, _P, _I, _I, _P]),
+    "ssn_cg_update": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_cg_next": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_inverse_from_cholesky": (_I, [_P, _P, _I, _I, _P]),
+    "ssn_spd_inverse": (_I, [_P, _P, _P, _I, _I, _P]),
+}
+
+SSN_OK = 0
+STATUS_NAMES = {0: "converged", 1: "invalid argument", 2: "CUDA error", 3: "Newton cap",
+                4: "line search", 5: "non-finite", 6: "eigh", 7: "workspace"}
+
+
+class Options(ctypes.Structure):
+    """ssn_options (include/ssn.h)."""
+    _fields_ = [("max_newton", ctypes.c_int), ("max_cg", ctypes.c_int),
+                ("max_backtrack", ctypes.c_int), ("feas_tol", ctypes.c_double),
+                ("reserved", ctypes.c_int * 8)]
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libssn.so once; raise if it is absent (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"native library {LIB_PATH} is missing; build it with "
+                "`python -c 'import __graft_entry__ as g; g.build()'` (nvcc, sm_100a)")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def options(max_newton=100, max_cg=150, max_backtrack=40, feas_tol=1e-8) -> Options:
+    opt = Options()
+    load().ssn_default_options(ctypes.byref(opt))
+    opt.max_newton, opt.max_cg, opt.max_backtrack, opt.feas_tol = max_newton, max_cg, max_backtrack, feas_tol
+    return opt
+
+
+def check(code: int, what: str) -> None:
+    if code != SSN_OK:
+        msg = load().ssn_status_string(code).decode()
+        raise RuntimeError(f"{what}: {msg} (status {code})")
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def require_cuda_f64(*tensors: torch.Tensor) -> torch.device:
+    dev = tensors[0].device
+    for t in tensors:
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float64 or t.device != dev:
+            raise ValueError("expected CUDA float64 tensors on one device")
+    return dev

@@ -1,0 +1,201 @@
+"""Batched dual Newton-CG solver: host side of the drop-in ``solve``.
+
+Mirrors src/symplectic_projection/dual_recommended_hvp.py of the reference:
+same constants, ``solve(T) -> (X, omega, iterations)`` for CPU float64 input
+(CPU output) and, additionally, CUDA input (device-resident output).  The
+pipeline Gram -> eigh -> Newton-CG -> recovery is one C-ABI call
+(``ssn_solve``) enqueued on torch's current stream; the host only checks the
+per-instance status words afterwards and raises ``RuntimeError`` for the whole
+batch on a Newton or line-search cap, as the reference does
+(dual_recommended_hvp.py:189-191).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+
+from . import _native as N
+from ._workspace import workspace
+
+# dual_recommended_hvp.py:13-19
+ROW_CHUNK = 1024
+DEVICE = "cuda"
+FEAS_TOL = 1e-8
+MAX_NEWTON, MAX_CG, MAX_BACKTRACK = 100, 150, 40
+PINNED_OUTPUT_MIN_BYTES = 64 * 2**20
+
+_MESSAGES = {
+    3: "batched Newton iteration cap reached",
+    4: "batched line search found no descent step",
+    6: "Jacobi eigensolver did not converge",
+}
+
+
+@dataclass
+class SolveResult:
+    """Extended result of :func:`solve_ex` (all tensors on the input's device)."""
+    X: torch.Tensor
+    omega: torch.Tensor
+    iterations: torch.Tensor
+    status: torch.Tensor        # int32 per instance: 0 converged, 3 Newton cap, 4 line search, 5 non-finite, 6 eigh
+
+
+def _check_target(T):
+    if not isinstance(T, torch.Tensor) or T.dtype != torch.float64:
+        raise ValueError("T must be a torch.float64 tensor; no implicit precision conversion")
+    if T.ndim != 3 or T.shape[-2] % 2 or T.shape[-1] % 2 or T.shape[-1] == 0:
+        raise ValueError("T must have shape [batch, 2n, 2k] with k >= 1")
+    batch, rows, m = T.shape
+    if m > 128:
+        raise ValueError("2k <= 128 is supported")
+    if rows < m:
+        raise ValueError("n >= k is required")
+    return batch, rows // 2, m
+
+
+def _pinned_like(T: torch.Tensor) -> torch.Tensor:
+    big = T.numel() * T.element_size() >= PINNED_OUTPUT_MIN_BYTES
+    return torch.empty(T.shape, dtype=T.dtype, pin_memory=big)
+
+
+@torch.no_grad()
+def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
+             max_backtrack: int = MAX_BACKTRACK, feas_tol: float = FEAS_TOL,
+             raise_on_failure: bool = False) -> SolveResult:
+    """Device-resident solve with per-instance status.  T must be a CUDA tensor."""
+    batch, n, m = _check_target(T)
+    dev = N.require_cuda_f64(T)
+    T = T.contiguous()
+    X = torch.empty_like(T)
+    omega = torch.empty(batch, m, m, dtype=torch.float64, device=dev)
+    iterations = torch.empty(batch, dtype=torch.int64, device=dev)
+    status = torch.empty(batch, dtype=torch.int32, device=dev)
+    if batch == 0:
+        return SolveResult(X, omega, iterations, status)
+    lib = N.load()
+    nbytes = lib.ssn_workspace_bytes(batch, n, m)
+    ws = workspace(dev, nbytes)
+    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol)
+    N.check(lib.ssn_solve(T.data_ptr(), X.data_ptr(), omega.data_ptr(), iterations.data_ptr(),
+                          status.data_ptr(), batch, n, m, ws.data_ptr(), nbytes,
+                          N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_solve")
+    if raise_on_failure:
+        raise_for_status(status)
+    return SolveResult(X, omega, iterations, status)
+
+
+def raise_for_status(status: torch.Tensor) -> None:
+    """Raise RuntimeError for the batch if any instance hit a cap (synchronises)."""
+    codes = status.cpu().tolist()
+    for code in (3, 4, 6):
+        if code in codes:
+            bad = [i for i, c in enumerate(codes) if c == code]
+            raise RuntimeError(f"{_MESSAGES[code]} (instances {bad[:8]}{'...' if len(bad) > 8 else ''})")
+
+
+@torch.no_grad()
+def solve(T: torch.Tensor, **options):
+    """(X, omega, iterations) for T float64 [batch, 2n, 2k] (dual_recommended_hvp.py:231-242).
+
+    CPU input -> CPU outputs (X pinned when >= 64 MiB, like the reference);
+    CUDA input -> CUDA outputs.  Raises RuntimeError for the whole batch on a
+    Newton or line-search cap.
+    """
+    _check_target(T)
+    if T.is_cuda:
+        res = solve_ex(T, **options)
+        raise_for_status(res.status)
+        return res.X, res.omega, res.iterations
+    dev = torch.device("cuda", torch.cuda.current_device())
+    Td = T.to(dev, non_blocking=T.is_pinned())
+    res = solve_ex(Td, **options)
+    raise_for_status(res.status)
+    X = _pinned_like(T)
+    X.copy_(res.X)
+    return X, res.omega.cpu(), res.iterations.cpu()
+
+
+# ---- lower-level pieces of the reference module -------------------------------------------
+@torch.no_grad()
+def gram_chunks(T, blocks=None):
+    """(Cr, Ci) on the device for T [batch, 2n, m] (dual_recommended_hvp.py:79-96).
+
+    The whole batch is copied once (no 1024-row staging); if ``blocks`` is a
+    list, the device copies of (A, D) are appended to it for recover_matmul.
+    """
+    from .gram_triangle_reflect import gram
+    batch, n, m = _check_target(T)
+    Td = T if T.is_cuda else T.to(DEVICE)
+    A, D = Td[:, :n], Td[:, n:]
+    if blocks is not None:
+        blocks.append((A, D))
+    return gram(A, D)
+
+
+@torch.no_grad()
+def eigh_scaled(Cr):
+    """(values, vectors, scale) with Cr/scale = V diag(values) V^T, scale = max(1, tr(Cr)/m).
+
+    Device Jacobi replacing torch.linalg.eigh at dual_recommended_hvp.py:106-108.
+    """
+    dev = N.require_cuda_f64(Cr)
+    batch, m, _ = Cr.shape
+    Cr = Cr.contiguous()
+    values = torch.empty(batch, m, dtype=torch.float64, device=dev)
+    vectors = torch.empty(batch, m, m, dtype=torch.float64, device=dev)
+    scale = torch.empty(batch, dtype=torch.float64, device=dev)
+    sweeps = torch.empty(batch, dtype=torch.int32, device=dev)
+    N.check(N.load().ssn_eigh(Cr.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(),
+                              sweeps.data_ptr(), batch, m, N.stream_handle(dev)), "ssn_eigh")
+    return values, vectors, scale, sweeps
+
+
+@torch.no_grad()
+def dual_batch(Cr, Ci, final=None, **options):
+    """(omega, L, iterations) from device Gram matrices (dual_recommended_hvp.py:99-191).
+
+    If ``final`` is a list it receives (P, Q), the cached inverse parts in the
+    original basis, like the reference.  L = chol(I + omega omega) is formed
+    with torch.linalg.cholesky only to keep the reference's return shape; the
+    solve path does not use it.
+    """
+    dev = N.require_cuda_f64(Cr, Ci)
+    batch, m, _ = Cr.shape
+    Cr, Ci = Cr.contiguous(), Ci.contiguous()
+    omega = torch.empty(batch, m, m, dtype=torch.float64, device=dev)
+    P, Q = torch.empty_like(omega), torch.empty_like(omega)
+    iterations = torch.empty(batch, dtype=torch.int64, device=dev)
+    status = torch.empty(batch, dtype=torch.int32, device=dev)
+    lib = N.load()
+    nbytes = lib.ssn_dual_workspace_bytes(batch, m)
+    ws = workspace(dev, nbytes)
+    opt = N.options(options.get("max_newton", MAX_NEWTON), options.get("max_cg", MAX_CG),
+                    options.get("max_backtrack", MAX_BACKTRACK), options.get("feas_tol", FEAS_TOL))
+    N.check(lib.ssn_dual(Cr.data_ptr(), Ci.data_ptr(), omega.data_ptr(), P.data_ptr(), Q.data_ptr(),
+                         iterations.data_ptr(), status.data_ptr(), batch, m, ws.data_ptr(), nbytes,
+                         N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_dual")
+    raise_for_status(status)
+    if final is not None:
+        final[:] = (P, Q)
+    eye = torch.eye(m, dtype=torch.float64, device=dev)
+    L = torch.linalg.cholesky(eye + omega @ omega)
+    return omega, L, iterations
+
+
+@torch.no_grad()
+def recover_matmul(T, omega, L, blocks=None, final=None):
+    """X for T using the cached (P, Q) in ``final`` (dual_recommended_hvp.py:194-228)."""
+    from .recovery_fused import recover_block
+    batch, n, m = _check_target(T)
+    if not final:
+        raise ValueError("final=(P, Q) from dual_batch is required")
+    P, Q = final
+    if blocks:
+        A, D = blocks[0]
+    else:
+        Td = T if T.is_cuda else T.to(P.device)
+        A, D = Td[:, :n], Td[:, n:]
+    Ur, Ui = recover_block(A, D, P, Q)
+    X = torch.cat((Ur, Ui), dim=1)
+    return X if T.is_cuda else X.cpu()

@@ -1,0 +1,39 @@
+"""Gram products of the stacked halves of T (gram_triangle_reflect.py:19-36)."""
+import torch
+
+from . import _native as N
+from ._workspace import workspace
+
+
+def initialize_kernels():
+    N.load()
+
+
+@torch.no_grad()
+def gram(A, D):
+    """Return (Cr, Ci) = (A^T A + D^T D, A^T D - D^T A) for CUDA float64 [batch, rows, m]."""
+    dev = N.require_cuda_f64(A, D)
+    batch, rows, m = A.shape
+    if D.shape != A.shape:
+        raise ValueError("A and D must have the same shape")
+    A, D = A.contiguous(), D.contiguous()
+    Cr = torch.empty(batch, m, m, dtype=torch.float64, device=dev)
+    Ci = torch.empty_like(Cr)
+    lib = N.load()
+    nbytes = lib.ssn_gram_workspace_bytes(batch, rows, m)
+    ws = workspace(dev, nbytes)
+    N.check(lib.ssn_gram(A.data_ptr(), D.data_ptr(), rows * m, Cr.data_ptr(), Ci.data_ptr(),
+                         batch, rows, m, ws.data_ptr(), nbytes, N.stream_handle(dev)), "ssn_gram")
+    return Cr, Ci
+
+
+@torch.no_grad()
+def gram_add_(A, D, Cr, Ci, split_diagonal=True):
+    """Cr += A.T@A + D.T@D; Ci += A.T@D - D.T@A (inputs and outputs must not alias)."""
+    batch, rows, m = A.shape
+    if D.shape != A.shape or Cr.shape != (batch, m, m) or Ci.shape != (batch, m, m):
+        raise ValueError("shape mismatch")
+    N.require_cuda_f64(A, D, Cr, Ci)
+    cr, ci = gram(A, D)
+    Cr.add_(cr)
+    Ci.add_(ci)
