@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Throughput of the batched FP64 dual Newton-CG symplectic Stiefel solver on B200.
+
+Workload: 64 seeded Gaussian targets T of 8192 x 96 (n = 4096, k = 48), entries
+N(0, 1/(2n)) from the reference protocol's generator rule; one step = one full
+batched solve (Gram -> eigh -> Newton-CG -> recovery), every instance must pass
+r_F <= 1e-8, r_G <= 1e-9, delta <= 1e-8 (checked on the device after timing).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU, each rank solving its own batch
+(weak scaling, no collective on the data path); the step time is the max over
+ranks.  ``--impl reference`` times the reference algorithm's CPU FP64 path (the
+CPU restatement in oracle/, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "symplectic-stiefel-nearness_b200"))
+
+METRIC = "solves/s, 64×(8192×96) batch, all pass r_F/r_G/δ checks: split-prec vs FP64"
+N_DEFAULT, K_DEFAULT, BATCH_DEFAULT = 4096, 48, 64
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=N_DEFAULT)
+    p.add_argument("--k", type=int, default=K_DEFAULT)
+    p.add_argument("--batch", type=int, default=BATCH_DEFAULT)
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(args):
+    return {"workload": f"{args.batch} x ({2 * args.n} x {2 * args.k}) FP64 targets, n={args.n}, k={args.k}",
+            "batch": args.batch, "n": args.n, "k": args.k, "precision": "fp64",
+            "inputs": "T resident in HBM, 403 MB > 126 MB L2 (no flush needed)"
+            if (args.n, args.k, args.batch) == (N_DEFAULT, K_DEFAULT, BATCH_DEFAULT)
+            else "T resident in HBM"}
+
+
+def make_targets(args, pin):
+    from symplectic_projection.inputs import case_index, gaussian_targets
+    try:
+        case = case_index(args.n, args.k)
+    except ValueError:
+        case = 0
+    return gaussian_targets(args.n, args.k, args.batch, case, pin_memory=pin)
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_baseline(args, seconds):
+    """The reference algorithm's CPU FP64 path (oracle restatement), all host threads."""
+    import torch
+    sys.path.insert(0, str(ROOT))
+    from oracle import ssn_oracle as O
+    T, _ = O.make_inputs(args.n, args.k, 5 if (args.n, args.k) == (4096, 48) else 0, args.batch)
+    threads = torch.get_num_threads()
+    O.solve(T[:2])                                   # warm-up (thread pool, allocator)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        O.solve(T)
+        done += T.shape[0]
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": done / el, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{done // T.shape[0]} full batched solve(s) of the {args.batch}-target workload, "
+                      f"{el:.1f} s, torch CPU FP64, {threads} threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import torch
+    sys.path.insert(0, str(ROOT))
+    from oracle import ssn_oracle as O
+    T, _ = O.make_inputs(args.n, args.k, 5 if (args.n, args.k) == (4096, 48) else 0, args.batch)
+    for _ in range(max(0, min(args.warmup, 1))):
+        O.solve(T)
+    times = []
+    steps = max(1, min(args.steps, 5))               # each step is a full batch: bounded run time
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.solve(T)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = args.batch * steps / total
+    threads = torch.get_num_threads()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * total / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded N(0,1/(2n)) targets (reference generator rule)",
+            "config": workload(args),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": f"{steps} full batched solves of {args.batch} targets on host CPU, "
+                                       f"oracle restatement of the reference algorithm, {threads} threads"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid, self.lines, self.proc = uuid, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", self.uuid], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import symplectic_projection as sp
+    from symplectic_projection import _native as N
+    from symplectic_projection.certify import certify
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    sp.initialize_kernels()
+    lib = N.load()
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    B, n, k = args.batch, args.n, args.k
+    m = 2 * k
+    T_host = make_targets(args, pin=True)
+    T = T_host.to(dev)
+    X = torch.empty_like(T)
+    Cr = torch.empty(B, m, m, dtype=torch.float64, device=dev)
+    Ci, omega, Pf, Qf, vectors = (torch.empty_like(Cr) for _ in range(5))
+    values = torch.empty(B, m, dtype=torch.float64, device=dev)
+    scale = torch.empty(B, dtype=torch.float64, device=dev)
+    sweeps = torch.empty(B, dtype=torch.int32, device=dev)
+    iters = torch.empty(B, dtype=torch.int64, device=dev)
+    status = torch.empty(B, dtype=torch.int32, device=dev)
+    counters = torch.zeros(B, 4, dtype=torch.int32, device=dev)
+    gram_bytes = lib.ssn_gram_workspace_bytes(B, n, m)
+    newton_bytes = lib.ssn_newton_workspace_bytes(B, m)
+    eigh_bytes = lib.ssn_eigh_workspace_bytes(B, m)
+    ws = torch.empty(max(gram_bytes, newton_bytes, eigh_bytes), dtype=torch.uint8, device=dev)
+    opt = N.options()
+    stride = 2 * n * m
+    A_ptr, D_ptr = T.data_ptr(), T.data_ptr() + 8 * n * m
+    X_top, X_bot = X.data_ptr(), X.data_ptr() + 8 * n * m
+
+    def phases(ev=None):
+        if ev: ev[0].record(stream)
+        N.check(lib.ssn_gram(A_ptr, D_ptr, stride, Cr.data_ptr(), Ci.data_ptr(), B, n, m,
+                             ws.data_ptr(), gram_bytes, sh), "gram")
+        if ev: ev[1].record(stream)
+        N.check(lib.ssn_eigh(Cr.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(),
+                             sweeps.data_ptr(), B, m, ws.data_ptr(), eigh_bytes, sh), "eigh")
+        if ev: ev[2].record(stream)
+        N.check(lib.ssn_newton(Ci.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(), None,
+                               omega.data_ptr(), Pf.data_ptr(), Qf.data_ptr(), iters.data_ptr(),
+                               status.data_ptr(), counters.data_ptr(), B, m, ws.data_ptr(), newton_bytes,
+                               N.ctypes.byref(opt), sh), "newton")
+        if ev: ev[3].record(stream)
+        N.check(lib.ssn_recover(A_ptr, D_ptr, stride, Pf.data_ptr(), Qf.data_ptr(), X_top, X_bot, stride,
+                                B, n, m, sh), "recover")
+        if ev: ev[4].record(stream)
+
+    # FP64 tensor-pipe peak on this GPU (denominator of the FP64 rooflines), best of 3
+    sink = torch.empty(8192, dtype=torch.float64, device=dev)
+    flops = N.ctypes.c_double(0.0)
+    peak = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        N.check(lib.ssn_probe_fp64_mma(sink.data_ptr(), 4000, N.ctypes.byref(flops), sh), "probe")
+        e1.record(stream)
+        e1.synchronize()
+        peak = max(peak, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+
+    for _ in range(max(3, args.warmup)):
+        phases()
+    torch.cuda.synchronize(dev)
+
+    K = args.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
+    sampler = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for s in range(K):
+        phases(evs[s])
+    end.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    total_ms = start.elapsed_time(end)
+    phase_ms = [0.0] * 4
+    for ev in evs:
+        for i in range(4):
+            phase_ms[i] += ev[i].elapsed_time(ev[i + 1])
+    if world > 1:
+        t = torch.tensor([total_ms] + phase_ms, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, phase_ms = float(t[0]), [float(x) for x in t[1:]]
+
+    # correctness of the timed outputs: every instance converged and passes the checks
+    st = status.cpu()
+    cert = certify(T, X)
+    passed = bool(cert["passed"].all()) and bool((st == 0).all())
+    worst = {key: float(cert[key].max()) for key in ("feasibility", "stationarity", "delta")}
+    cnt = counters.cpu().to(torch.int64)
+
+    # algorithmic work per launch
+    n_steps, n_hvp, n_trial = (int(cnt[:, i].sum()) for i in range(3))
+    mm3 = 2.0 * m ** 3
+    newton_flops = (4 * n_hvp + 7 * max(0, n_steps - B) + 6 * n_trial + 9 * B) * mm3
+    tall_flops = 8.0 * n * m * m * B             # per Gram or per recovery launch
+    per_launch = {"gram": (tall_flops, phase_ms[0] / K), "eigh": (None, phase_ms[1] / K),
+                  "newton": (newton_flops, phase_ms[2] / K), "recover": (tall_flops, phase_ms[3] / K)}
+    dominant = max(per_launch, key=lambda kk: per_launch[kk][1])
+    fl, ms = per_launch[dominant]
+    achieved = (fl / (ms * 1e-3) / 1e12) if fl else None
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None, "kernel": dominant,
+                "peak_source": "FP64 DMMA rate measured in this run (ssn_probe_fp64_mma); "
+                               "no FP64 figure in the driver's peak file"}
+    phases_out = {}
+    for name, (f, t_ms) in per_launch.items():
+        phases_out[name] = {"ms": t_ms, "tflops": (f / (t_ms * 1e-3) / 1e12) if f else None,
+                            "frac_of_fp64_peak": (f / (t_ms * 1e-3) / 1e12 / peak) if f else None}
+    phases_out["newton"]["work"] = {"newton_steps": n_steps, "hvps": n_hvp, "trials": n_trial,
+                                    "algorithmic_flops": newton_flops}
+    sw = sweeps.cpu()
+    phases_out["eigh"]["jacobi_sweeps"] = {"max": int(sw.max()), "mean": float(sw.double().mean())}
+    phases_out["hbm_floor_ms"] = 48.0 * n * m * B / 6549.8e9 * 1e3
+
+    ms_step = total_ms / K
+    value = world * B / (ms_step * 1e-3)
+
+    # end to end through the public API: pinned host T -> device -> host X, omega, iterations
+    e2e_ms = []
+    X_host = None
+    for i in range(1 + max(1, args.e2e_steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        X_host, W_host, I_host = sp.solve(T_host)
+        e1.record(stream)
+        e1.synchronize()
+        if i > 0:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_step = sum(e2e_ms) / max(1, len(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_step], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t[0])
+    h2d = T_host.numel() * 8
+    d2h = X_host.numel() * 8 + W_host.numel() * 8 + I_host.numel() * 8 + B * 4
+    # raw pinned copy rates of this host link (the floor of the end-to-end number)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    T.copy_(T_host, non_blocking=True)
+    e1.record(stream)
+    X_host.copy_(X, non_blocking=True)
+    e2.record(stream)
+    e2.synchronize()
+    link = {"h2d_gbs": h2d / (e0.elapsed_time(e1) * 1e-3) / 1e9,
+            "d2h_gbs": X.numel() * 8 / (e1.elapsed_time(e2) * 1e-3) / 1e9}
+
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": K,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded N(0,1/(2n)) targets (reference generator rule)",
+            "config": dict(workload(args), precision="fp64 (plain FP64 form)", parallelism=f"replicas x{world}"),
+            "all_pass": passed, "worst": worst, "clocks": clocks,
+            "e2e": {"value": world * B / (e2e_step * 1e-3), "unit": "solves/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step,
+                    "link": link},
+            "gpu_launches": 6 * K, "roofline": roofline, "phases": phases_out}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0 if passed else 1
+
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -76,8 +76,9 @@ size_t ssn_workspace_bytes(int batch, int n, int m);
  * Replaces symplectic_projection.solve (dual_recommended_hvp.py:231-242),
  * i.e. gram_chunks (:79-96) + dual_batch (:99-191) + recover_matmul (:194-228),
  * with device-resident input and output (no chunked PCIe staging).
- * Returns SSN_OK when every instance converged, else the first failing
- * instance's code (the reference raises RuntimeError for the whole batch).
+ * Returns SSN_OK when the work was enqueued; per-instance outcomes are in
+ * `status` once the stream reaches them (the reference raises RuntimeError
+ * for the whole batch when any instance hits a cap; the Python layer does).
  */
 int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations,
               int32_t* status, int batch, int n, int m,
@@ -110,11 +111,13 @@ int ssn_recover(const double* A, const double* D, int64_t ab_stride,
  * Symmetric eigendecomposition of the scaled Gram matrix, Cr / s = V diag(w) V^T
  * with s = max(1, trace(Cr)/m) (dual_recommended_hvp.py:106-108, where the
  * reference calls torch.linalg.eigh).  Cyclic two-sided Jacobi in FP64;
- * eigenvalues ascending.  scale may be NULL.  sweeps (may be NULL) receives
- * the number of Jacobi sweeps per instance.
+ * eigenvalues ascending.  scale and sweeps (Jacobi sweeps per instance) may be
+ * NULL.  The workspace (ssn_eigh_workspace_bytes) holds the rotation log.
  */
+size_t ssn_eigh_workspace_bytes(int batch, int m);
 int ssn_eigh(const double* Cr, double* values, double* vectors, double* scale,
-             int32_t* sweeps, int batch, int m, ssn_stream_t stream);
+             int32_t* sweeps, int batch, int m, void* workspace, size_t workspace_bytes,
+             ssn_stream_t stream);
 
 /*
  * Dual Newton-CG on given Gram matrices: (Cr, Ci) -> omega, and the final
@@ -127,6 +130,30 @@ int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, doubl
              int64_t* iterations, int32_t* status, int batch, int m,
              void* workspace, size_t workspace_bytes, const ssn_options* opt,
              ssn_stream_t stream);
+
+/*
+ * The Newton-CG part of ssn_dual alone, given the eigendecomposition from
+ * ssn_eigh (values, vectors, scale, and its per-instance status eig_status,
+ * which may be NULL).  counters (may be NULL) receives int32 [batch, 4]:
+ * Newton steps run, Hessian-vector products, line-search trials, fallbacks.
+ * Replaces dual_batch (dual_recommended_hvp.py:109-191) after the eigh call.
+ * Needs ssn_newton_workspace_bytes.
+ */
+size_t ssn_newton_workspace_bytes(int batch, int m);
+int ssn_newton(const double* Ci, const double* values, const double* vectors, const double* scale,
+               const int32_t* eig_status, double* omega, double* P, double* Q,
+               int64_t* iterations, int32_t* status, int32_t* counters, int batch, int m,
+               void* workspace, size_t workspace_bytes, const ssn_options* opt,
+               ssn_stream_t stream);
+
+/*
+ * Measurement helper with no counterpart in the reference: launches a
+ * dependent-chain-free FP64 DMMA loop on every SM so a caller can time the
+ * FP64 tensor-pipe peak with its own events (the roofline denominator of the
+ * FP64 kernels).  sink: device buffer of >= 8192 doubles.  *flops receives the
+ * FP64 flops the launch performs.
+ */
+int ssn_probe_fp64_mma(double* sink, int iters, double* flops, ssn_stream_t stream);
 
 /* ---- component operations (mirrors of the reference kernel wrappers) ----
  * All matrices [batch, m, m] contiguous FP64; vectors [batch] or [batch, m]. */

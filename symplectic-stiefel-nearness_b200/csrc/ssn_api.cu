@@ -24,7 +24,7 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Workspace layout of ssn_solve (byte offsets, 256-byte aligned sections).
 struct SolveLayout {
-  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, total;
+  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, eig_ws, total;
 };
 
 SolveLayout solve_layout(int batch, int n, int m) {
@@ -48,12 +48,13 @@ SolveLayout solve_layout(int batch, int n, int m) {
   const size_t partial = sizeof(double) * gram_partial_doubles(batch, n, m);
   L.work = take(work > partial ? work : partial);
   L.eig_status = take(sizeof(int32_t) * batch);
+  L.eig_ws = take(eigh_workspace_bytes(batch, m));
   L.total = off;
   return L;
 }
 
 struct DualLayout {
-  size_t values, vectors, scale, work, eig_status, total;
+  size_t values, vectors, scale, work, eig_status, eig_ws, total;
 };
 
 DualLayout dual_layout(int batch, int m) {
@@ -70,6 +71,7 @@ DualLayout dual_layout(int batch, int m) {
   L.scale = take(sizeof(double) * batch);
   L.work = take(sizeof(double) * (size_t)batch * kDualMats * mm);
   L.eig_status = take(sizeof(int32_t) * batch);
+  L.eig_ws = take(eigh_workspace_bytes(batch, m));
   L.total = off;
   return L;
 }
@@ -151,7 +153,7 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
   const double* D = T + (size_t)n * m;
   cudaError_t e = launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
-  e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m, stream);
+  e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m, ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   DualArgs a{};
   a.m = m;
@@ -203,10 +205,17 @@ int ssn_recover(const double* A, const double* D, int64_t ab_stride, const doubl
                                     reinterpret_cast<cudaStream_t>(stream)));
 }
 
+size_t ssn_eigh_workspace_bytes(int batch, int m) {
+  if (!shape_ok(batch, m)) return 0;
+  return eigh_workspace_bytes(batch, m);
+}
+
 int ssn_eigh(const double* Cr, double* values, double* vectors, double* scale, int32_t* sweeps,
-             int batch, int m, ssn_stream_t stream) {
+             int batch, int m, void* workspace, size_t workspace_bytes, ssn_stream_t stream) {
   if (!shape_ok(batch, m) || !Cr || !values || !vectors) return SSN_ERR_INVALID_ARGUMENT;
-  return cuda_status(launch_eigh(Cr, values, vectors, scale, sweeps, nullptr, batch, m,
+  if (!workspace || workspace_bytes < eigh_workspace_bytes(batch, m) || !aligned16(workspace))
+    return SSN_ERR_WORKSPACE;
+  return cuda_status(launch_eigh(Cr, values, vectors, scale, sweeps, nullptr, batch, m, workspace,
                                  reinterpret_cast<cudaStream_t>(stream)));
 }
 
@@ -229,7 +238,8 @@ int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, doubl
   double* vectors = reinterpret_cast<double*>(ws + L.vectors);
   double* scale = reinterpret_cast<double*>(ws + L.scale);
   int32_t* eig_status = reinterpret_cast<int32_t*>(ws + L.eig_status);
-  cudaError_t e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m, stream);
+  cudaError_t e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m,
+                              ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   DualArgs a{};
   a.m = m;
@@ -248,6 +258,44 @@ int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, doubl
   a.status = status;
   a.counters = nullptr;
   return cuda_status(launch_dual(a, batch, stream));
+}
+
+size_t ssn_newton_workspace_bytes(int batch, int m) {
+  if (!shape_ok(batch, m)) return 0;
+  return sizeof(double) * (size_t)batch * kDualMats * m * m;
+}
+
+int ssn_newton(const double* Ci, const double* values, const double* vectors, const double* scale,
+               const int32_t* eig_status, double* omega, double* P, double* Q, int64_t* iterations,
+               int32_t* status, int32_t* counters, int batch, int m, void* workspace,
+               size_t workspace_bytes, const ssn_options* opt, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !Ci || !values || !vectors || !scale || !omega || !P || !Q ||
+      !iterations || !status || !options_ok(opt) || !aligned16(Ci) || !aligned16(vectors))
+    return SSN_ERR_INVALID_ARGUMENT;
+  if (!workspace || workspace_bytes < ssn_newton_workspace_bytes(batch, m) || !aligned16(workspace))
+    return SSN_ERR_WORKSPACE;
+  DualArgs a{};
+  a.m = m;
+  fill_options(opt, a);
+  a.Cr = nullptr;
+  a.Ci = Ci;
+  a.values = values;
+  a.vectors = vectors;
+  a.scale = scale;
+  a.eig_status = eig_status;
+  a.work = static_cast<double*>(workspace);
+  a.omega = omega;
+  a.P = P;
+  a.Q = Q;
+  a.iterations = iterations;
+  a.status = status;
+  a.counters = counters;
+  return cuda_status(launch_dual(a, batch, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_probe_fp64_mma(double* sink, int iters, double* flops, ssn_stream_t stream) {
+  if (!sink || !flops || iters < 1 || iters > (1 << 24)) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_probe_fp64_mma(sink, iters, flops, reinterpret_cast<cudaStream_t>(stream)));
 }
 
 #define SSN_CHECK_MATS(...)                                                   \

@@ -293,3 +293,128 @@ __host__ __device__ constexpr int slot_doubles_rows(int rows, int MB) {
 }
 
 }  // namespace ssn
+
+namespace ssn {
+
+// ---------------------------------------------------------------- shared-memory products
+// out(i, j) for i < R, j < N of op(A)[R x K] * op(B)[K x N] with both operands
+// already in shared memory (row-major, leading dims lda/ldb, K a multiple of 4,
+// R and N multiples of 8).  Each warp computes 16 x 16 output blocks (2 x 2
+// DMMA tiles) in turn and hands every element to fn(i, j, value).  No barrier.
+// Leading dimensions == 4 (mod 16) keep the fragment loads conflict-free.
+template <bool AT, bool BT, class Fn>
+__device__ __forceinline__ void smem_product(int R, int N, int K, const double* A, int lda,
+                                             const double* B, int ldb, Fn&& fn) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int br = cdiv(R, 16), bc = cdiv(N, 16);
+  for (int blk = warp; blk < br * bc; blk += nwarps) {
+    const int r0 = (blk / bc) * 16, c0 = (blk % bc) * 16;
+    double acc[2][2][2] = {};
+    for (int k = 0; k < K; k += 4) {
+      double af[2], bf[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = r0 + 8 * i + g;
+        af[i] = (r0 + 8 * i < R) ? (AT ? A[(k + t) * lda + r] : A[r * lda + k + t]) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int c = c0 + 8 * j + g;
+        bf[j] = (c0 + 8 * j < N) ? (BT ? B[c * ldb + k + t] : B[(k + t) * ldb + c]) : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = r0 + 8 * i + g, c = c0 + 8 * j + 2 * t + e;
+          if (r0 + 8 * i < R && c0 + 8 * j < N) fn(r, c, acc[i][j][e]);
+        }
+  }
+}
+
+// Inverse of a symmetric positive definite matrix held in shared memory,
+// in place, by block Gauss-Jordan sweeps over 16 x 16 pivot blocks:
+//   Dinv = K_PP^-1,  U = Dinv K_PQ,  W = K_QP Dinv,
+//   K_QQ -= K_QP U,  K_PQ = U,  K_QP = -W,  K_PP = Dinv,
+// for each pivot block P (Q = the other indices).  The small inverse is a
+// scalar sweep run by warp 0 whose pivots are the Schur-complement diagonals:
+// they are all positive exactly when K is positive definite (the test
+// torch.linalg.cholesky_ex applies).  K: mp x mp (mp = m rounded up to 16;
+// the caller pads the tail with the identity), leading dim ld == 4 (mod 16).
+// scratch: 16 * ld + mp * 20 doubles.  Returns the same bool in every thread.
+__host__ __device__ constexpr int spd_region_doubles(int m) {
+  return round_up(m, 16) * frag_ld(round_up(m, 16)) + 16 * frag_ld(round_up(m, 16)) + round_up(m, 16) * 20;
+}
+
+__device__ __forceinline__ bool spd_inverse_blocked(double* K, int mp, int ld, double* scratch,
+                                                    int* flag) {
+  constexpr int b = 16;
+  double* U = scratch;               // b x ld   : U[p][j]
+  double* W = scratch + b * ld;      // mp x b   stored as W[j][p] with leading dim 20
+  if (threadIdx.x == 0) *flag = 1;
+  for (int k0 = 0; k0 < mp; k0 += b) {
+    // (1) warp 0 inverts the b x b diagonal block in place (scalar sweep operator)
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      bool ok = true;
+      for (int k = 0; k < b; ++k) {
+        __syncwarp();
+        const double piv = K[(k0 + k) * ld + k0 + k];
+        if (!(piv > 0.0) || !isfinite(piv)) { ok = false; break; }
+        const double inv = 1.0 / piv;
+        // each lane owns row i = lane & 15, columns j = (lane >> 4) * 8 + 0..7
+        const int i = lane & 15, jb = (lane >> 4) * 8;
+        const double aik = K[(k0 + i) * ld + k0 + k];
+        double rowk[8];
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) rowk[jj] = K[(k0 + k) * ld + k0 + jb + jj];
+        __syncwarp();
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int j = jb + jj;
+          double v;
+          if (i == k) v = (j == k) ? inv : rowk[jj] * inv;
+          else if (j == k) v = -aik * inv;
+          else v = K[(k0 + i) * ld + k0 + j] - aik * (rowk[jj] * inv);
+          K[(k0 + i) * ld + k0 + j] = v;
+        }
+      }
+      __syncwarp();
+      if (lane == 0 && !ok) *flag = 0;
+    }
+    __syncthreads();
+    if (*flag == 0) return false;
+    // (2) U = Dinv K_P,:  and  W = K_:,P Dinv  (P columns/rows skipped later)
+    const double* Dinv = K + k0 * ld + k0;
+    smem_product<false, false>(b, mp, b, Dinv, ld, K + k0 * ld, ld,
+                               [&](int p, int j, double v) { U[p * ld + j] = v; });
+    smem_product<false, false>(mp, b, b, K + k0, ld, Dinv, ld,
+                               [&](int j, int p, double v) { W[j * 20 + p] = v; });
+    __syncthreads();
+    // (3) K_QQ -= K_QP U   (rows/cols of P are rewritten in (4))
+    smem_product<false, false>(mp, mp, b, K + k0, ld, U, ld, [&](int i, int j, double v) {
+      const bool in_p = (i >= k0 && i < k0 + b) || (j >= k0 && j < k0 + b);
+      if (!in_p) K[i * ld + j] -= v;
+    });
+    __syncthreads();
+    // (4) K_PQ = U, K_QP = -W
+    for (int e = threadIdx.x; e < b * mp; e += blockDim.x) {
+      const int p = e / mp, j = e - p * mp;
+      if (j >= k0 && j < k0 + b) continue;
+      K[(k0 + p) * ld + j] = U[p * ld + j];
+      K[j * ld + k0 + p] = -W[j * 20 + p];
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+}  // namespace ssn

@@ -37,48 +37,6 @@ constexpr uint32_t C_DIFF = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 2);
 constexpr uint32_t C_CPLX = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1) | coef_bit(1, 1, 0, 1) |
                             coef_bit(1, 0, 1, 2);
 
-// In-place Gauss-Jordan inversion of an SPD matrix held in shared memory
-// (ld = m + 1).  Pivot k uses the current Schur complement diagonal, which is
-// positive for every k exactly when the matrix is positive definite -- the
-// same test torch.linalg.cholesky_ex applies.  Returns false (uniformly) on a
-// non-positive or non-finite pivot.  vec: 4*m doubles of scratch.  One CTA
-// barrier per pivot: the next pivot row/column are written to a second buffer.
-__device__ bool spd_inverse_smem(double* K, int m, double* vec) {
-  const int ld = m + 1;
-  double* rowv[2] = {vec, vec + m};
-  double* colv[2] = {vec + 2 * m, vec + 3 * m};
-  for (int j = threadIdx.x; j < m; j += blockDim.x) {
-    rowv[0][j] = K[j];
-    colv[0][j] = K[j * ld];
-  }
-  __syncthreads();
-  const int mm = m * m;
-  for (int k = 0; k < m; ++k) {
-    const int cur = k & 1, nxt = cur ^ 1;
-    const double piv = rowv[cur][k];
-    if (!(piv > 0.0) || !isfinite(piv)) return false;
-    const double inv = 1.0 / piv;
-    const double* rk = rowv[cur];
-    const double* ck = colv[cur];
-    for (int e = threadIdx.x; e < mm; e += blockDim.x) {
-      const int i = e / m, j = e - i * m;
-      double v;
-      if (i == k) {
-        v = (j == k) ? inv : rk[j] * inv;
-      } else if (j == k) {
-        v = -ck[i] * inv;
-      } else {
-        v = K[i * ld + j] - ck[i] * (rk[j] * inv);
-      }
-      K[i * ld + j] = v;
-      if (i == k + 1) rowv[nxt][j] = v;
-      if (j == k + 1) colv[nxt][i] = v;
-    }
-    __syncthreads();
-  }
-  return true;
-}
-
 template <int MB>
 struct Dual {
   int m, mm;
@@ -92,50 +50,69 @@ struct Dual {
   }
 };
 
+// Element loops without integer division: warp w owns rows w, w+16, ..., lane l
+// owns columns l, l+32, ...; consecutive lanes touch consecutive addresses.
+#define SSN_FOR_IJ(m_, BODY)                                                          \
+  for (int i = (int)(threadIdx.x >> 5); i < (m_); i += kWarps)                        \
+    for (int j = (int)(threadIdx.x & 31); j < (m_); j += 32) {                        \
+      const int e = i * (m_) + j;                                                     \
+      (void)e;                                                                        \
+      BODY                                                                            \
+    }
+
 template <int MB>
 __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   extern __shared__ __align__(16) double smem[];
   const int inst = blockIdx.x;
-  const int m = a.m, mm = m * m, tid = threadIdx.x;
+  const int m = a.m, mm = m * m;
   const int slot = slot_doubles(MB);
-  double* red = smem + 8 * slot;              // 2*kWarps doubles
+  const int region = imax(8 * slot, spd_region_doubles(m));
+  double* red = smem + region;                // 2*kWarps doubles
   double* lam = red + 2 * kWarps;             // m doubles
+  int* flag = reinterpret_cast<int*>(lam + kMaxM);
+  double* Zs = smem;                          // m x (m+1): HVP outer product, after the engine
+  const int zld = m + 1;
   Dual<MB> eng{m, mm, smem, slot};
 
   double* ws = a.work + (size_t)inst * kDualMats * mm;
-  double* buf[kDualMats];
-#pragma unroll
-  for (int k = 0; k < kDualMats; ++k) buf[k] = ws + (size_t)k * mm;
   const double* Ci = a.Ci + (size_t)inst * mm;
   const double* V = a.vectors + (size_t)inst * mm;
   const double s = a.scale[inst];
   int status = a.eig_status ? a.eig_status[inst] : SSN_INSTANCE_CONVERGED;
-  for (int i = tid; i < m; i += kThreads) lam[i] = a.values[(size_t)inst * m + i];
+  for (int i = threadIdx.x; i < m; i += kThreads) lam[i] = a.values[(size_t)inst * m + i];
   __syncthreads();
 
-  double *Ce = buf[M_CE], *Je = buf[M_JE], *Wm = buf[M_W], *Wt = buf[M_WT];
-  double *Pm = buf[M_P], *Pt = buf[M_PT], *Qm = buf[M_Q], *Sr = buf[M_SR], *Si = buf[M_SI];
-  double *G = buf[M_G], *Dd = buf[M_D], *Rr = buf[M_R], *Pp = buf[M_PP], *Hp = buf[M_HP];
-  double *Dl = buf[M_DL], *T1 = buf[M_T1], *T2 = buf[M_T2], *T3 = buf[M_T3];
+  double* Ce = ws + (size_t)M_CE * mm;
+  double* Je = ws + (size_t)M_JE * mm;
+  double* Wm = ws + (size_t)M_W * mm;
+  double* Wt = ws + (size_t)M_WT * mm;
+  double* Pm = ws + (size_t)M_P * mm;
+  double* Pt = ws + (size_t)M_PT * mm;
+  double* Qm = ws + (size_t)M_Q * mm;
+  double* Sr = ws + (size_t)M_SR * mm;
+  double* Si = ws + (size_t)M_SI * mm;
+  double* G = ws + (size_t)M_G * mm;
+  double* Dd = ws + (size_t)M_D * mm;
+  double* Rr = ws + (size_t)M_R * mm;
+  double* Pp = ws + (size_t)M_PP * mm;
+  double* Dl = ws + (size_t)M_DL * mm;
+  double* T1 = ws + (size_t)M_T1 * mm;
+  double* T2 = ws + (size_t)M_T2 * mm;
+  double* T3 = ws + (size_t)M_T3 * mm;
 
   auto store_to = [&](double* dst) {
     return [dst, m](int, int i, int j, double v) { dst[i * m + j] = v; };
-  };
-  auto precond = [&](const double* R, int i, int j) -> double {
-    const double x = __ddiv_rn(R[i * m + j], lam[i] + lam[j]);
-    const double y = __ddiv_rn(R[j * m + i], lam[j] + lam[i]);
-    return __dmul_rn(__dsub_rn(x, y), 0.5);
   };
 
   int64_t iterations = 0;
   int n_hvp = 0, n_trial = 0, n_fallback = 0, n_step = 0;
   if (status == SSN_INSTANCE_CONVERGED) {
     // ---- eigenbasis set-up: Ce = skew(V^T (Ci/s) V), Je = skew(V^T J(V)) / s  (:106-111, :53-56)
-    for (int e = tid; e < mm; e += kThreads) T1[e] = Ci[e] / s;
-    for (int e = tid; e < mm; e += kThreads) {
-      const int i = e / m, j = e - i * m, h = m / 2;
+    const int h = m / 2;
+    SSN_FOR_IJ(m, {
+      T1[e] = Ci[e] / s;
       T3[e] = i < h ? V[(i + h) * m + j] : -V[(i - h) * m + j];
-    }
+    })
     __syncthreads();
     {
       MatOp A[1] = {op_t(V, m)};
@@ -149,15 +126,18 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       auto epi = store_to(T1);
       eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
     }
-    for (int e = tid; e < mm; e += kThreads) {
-      const int i = e / m, j = e - i * m;
-      Ce[e] = (T1[e] - T1[j * m + i]) / 2;
-      Je[e] = ((Dl[e] - Dl[j * m + i]) / 2) / s;
+    // Skew parts are exactly antisymmetric ((x - y)/2 vs (y - x)/2), which every
+    // later pass relies on: precondition(r) = r / den and skew(w + t d) = w + t d
+    // hold bit for bit for exactly skew r, w, d.
+    SSN_FOR_IJ(m, {
+      const int et = j * m + i;
+      Ce[e] = (T1[e] - T1[et]) / 2;
+      Je[e] = ((Dl[e] - Dl[et]) / 2) / s;
       Wm[e] = 0.0;
       Pm[e] = (i == j) ? 1.0 : 0.0;
       Qm[e] = 0.0;
       Sr[e] = (i == j) ? lam[i] : 0.0;
-    }
+    })
     __syncthreads();
 
     const double sqrt_m = sqrt(static_cast<double>(m));
@@ -188,40 +168,29 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
         {
           MatOp A[2] = {op_n(T1, m), op_n(T2, m)};
           MatOp B[2] = {op_t(Pm, m), op_t(Qm, m)};
-          auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Sr : Si)[i * m + j] = v; };
+          auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T3 : Dl)[i * m + j] = v; };
           eng.template mul<2, 2, 2, C_CPLX>(A, B, epi);
         }
         SiCur = Si;
       }
       // Sr = sym, Si = skew, gradient = Je - Si and its norm (:126-128)
       double gn2 = 0.0;
-      for (int e = tid; e < mm; e += kThreads) {
-        const int i = e / m, j = e - i * m;
-        if (i > j) continue;
-        const int et = j * m + i;
-        double sij, sji;
-        if (step > 0) {
-          const double r = (Sr[e] + Sr[et]) / 2;
-          Sr[e] = r;
-          Sr[et] = r;
-          const double x = (Si[e] - Si[et]) / 2;
-          const double y = (Si[et] - Si[e]) / 2;
+      if (step > 0) {
+        SSN_FOR_IJ(m, {
+          const int et = j * m + i;
+          Sr[e] = (T3[e] + T3[et]) / 2;
+          const double x = (Dl[e] - Dl[et]) / 2;
           Si[e] = x;
-          Si[et] = y;
-          sij = x;
-          sji = y;
-        } else {
-          sij = Ce[e];
-          sji = Ce[et];
-        }
-        const double gij = Je[e] - sij;
-        G[e] = gij;
-        gn2 += gij * gij;
-        if (i != j) {
-          const double gji = Je[et] - sji;
-          G[et] = gji;
-          gn2 += gji * gji;
-        }
+          const double gij = Je[e] - x;
+          G[e] = gij;
+          gn2 += gij * gij;
+        })
+      } else {
+        SSN_FOR_IJ(m, {
+          const double gij = Je[e] - Ce[e];
+          G[e] = gij;
+          gn2 += gij * gij;
+        })
       }
       const double gnorm = sqrt(block_sum(gn2, red));
       const double residual = gnorm * s / sqrt_m;
@@ -232,38 +201,32 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       }
       ++iterations;
 
-      // ---- search direction
+      // ---- search direction.  g is exactly skew, so precondition(-g) = -g / den.
       double slope;
       if (step == 0) {
         // one preconditioner application solves H(E) = E L + L E exactly (:138-140)
         double sl = 0.0;
-        for (int e = tid; e < mm; e += kThreads) {
-          const int i = e / m, j = e - i * m;
-          const double x = __ddiv_rn(-G[e], lam[i] + lam[j]);
-          const double y = __ddiv_rn(-G[j * m + i], lam[j] + lam[i]);
-          const double z = __dmul_rn(__dsub_rn(x, y), 0.5);
+        SSN_FOR_IJ(m, {
+          const double z = __ddiv_rn(-G[e], lam[i] + lam[j]);
           Dd[e] = z;
           sl += G[e] * z;
-        }
+        })
         slope = block_sum(sl, red);
       } else {
         // PCG (:142-161)
-        for (int e = tid; e < mm; e += kThreads) {
-          Rr[e] = -G[e];
-          Dd[e] = 0.0;
-        }
-        __syncthreads();
         double rz = 0.0;
-        for (int e = tid; e < mm; e += kThreads) {
-          const int i = e / m, j = e - i * m;
-          const double z = precond(Rr, i, j);
+        SSN_FOR_IJ(m, {
+          const double r = -G[e];
+          const double z = __ddiv_rn(r, lam[i] + lam[j]);
+          Rr[e] = r;
+          Dd[e] = 0.0;
           Pp[e] = z;
-          rz += Rr[e] * z;
-        }
+          rz += r * z;
+        })
         rz = block_sum(rz, red);
         const double tol = fmin(fmax(sqrt(residual), 1e-8), 0.1) * gnorm;
         for (int it = 0; it < a.max_cg; ++it) {
-          // Hp = H(p): U = p Sr, V = p Si; Z = P U - Q V; Hp = Z - Z^T (:74-76)
+          // H(p) = Z - Z^T with Z = P (p Sr) - Q (p Si) (:74-76); Z stays in shared memory
           {
             MatOp A[1] = {op_n(Pp, m)};
             MatOp B[2] = {op_n(Sr, m), op_n(Si, m)};
@@ -273,58 +236,46 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           {
             MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
             MatOp B[2] = {op_n(T1, m), op_n(T2, m)};
-            auto epi = store_to(T3);
+            auto epi = [&](int, int i, int j, double v) { Zs[i * zld + j] = v; };
             eng.template mul<2, 2, 1, C_DIFF>(A, B, epi);
           }
           ++n_hvp;
           double curv = 0.0;
-          for (int e = tid; e < mm; e += kThreads) {
-            const int i = e / m, j = e - i * m;
-            const double h = T3[e] - T3[j * m + i];
-            Hp[e] = h;
-            curv += Pp[e] * h;
-          }
+          SSN_FOR_IJ(m, { curv += Pp[e] * (Zs[i * zld + j] - Zs[j * zld + i]); })
           curv = block_sum(curv, red);
           if (!(curv > 0.0)) break;  // cg_active &= curvature > 0 (:152)
           const double alpha = rz / curv;
-          double rn2 = 0.0;
-          for (int e = tid; e < mm; e += kThreads) {
+          double rn2 = 0.0, rz_next = 0.0;
+          SSN_FOR_IJ(m, {
+            const double hp = Zs[i * zld + j] - Zs[j * zld + i];
             Dd[e] = __dadd_rn(Dd[e], __dmul_rn(alpha, Pp[e]));
-            const double r = __dsub_rn(Rr[e], __dmul_rn(alpha, Hp[e]));
+            const double r = __dsub_rn(Rr[e], __dmul_rn(alpha, hp));
             Rr[e] = r;
             rn2 += r * r;
-          }
-          const double rnorm = sqrt(block_sum(rn2, red));
+            rz_next += r * __ddiv_rn(r, lam[i] + lam[j]);
+          })
+          block_sum2(rn2, rz_next, red);
+          const double rnorm = sqrt(rn2);
           if (!(rnorm > tol)) break;  // (:155-157)
-          double rz_next = 0.0;
-          for (int e = tid; e < mm; e += kThreads) {
-            const int i = e / m, j = e - i * m;
-            rz_next += Rr[e] * precond(Rr, i, j);
-          }
-          rz_next = block_sum(rz_next, red);
           const double beta = rz_next / rz;
-          for (int e = tid; e < mm; e += kThreads) {
-            const int i = e / m, j = e - i * m;
-            Pp[e] = __dadd_rn(precond(Rr, i, j), __dmul_rn(beta, Pp[e]));
-          }
+          SSN_FOR_IJ(m, {
+            Pp[e] = __dadd_rn(__ddiv_rn(Rr[e], lam[i] + lam[j]), __dmul_rn(beta, Pp[e]));
+          })
           __syncthreads();
           rz = rz_next;
         }
         double sl = 0.0;
-        for (int e = tid; e < mm; e += kThreads) sl += G[e] * Dd[e];
+        SSN_FOR_IJ(m, { sl += G[e] * Dd[e]; })
         slope = block_sum(sl, red);
         // non-descent fallback to the preconditioned gradient (:163-164)
         if (slope >= 0.0) {
           ++n_fallback;
           double s2 = 0.0;
-          for (int e = tid; e < mm; e += kThreads) {
-            const int i = e / m, j = e - i * m;
-            const double x = __ddiv_rn(-G[e], lam[i] + lam[j]);
-            const double y = __ddiv_rn(-G[j * m + i], lam[j] + lam[i]);
-            const double z = __dmul_rn(__dsub_rn(x, y), 0.5);
+          SSN_FOR_IJ(m, {
+            const double z = __ddiv_rn(-G[e], lam[i] + lam[j]);
             Dd[e] = z;
             s2 += G[e] * z;
-          }
+          })
           slope = block_sum(s2, red);
         }
       }
@@ -335,19 +286,16 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       for (int bt = 0; bt < a.max_backtrack; ++bt) {
         ++n_trial;
         double first = 0.0;
-        for (int e = tid; e < mm; e += kThreads) {
-          const int i = e / m, j = e - i * m, et = j * m + i;
+        SSN_FOR_IJ(m, {
           const double dl = __dmul_rn(t, Dd[e]);
           Dl[e] = dl;
           first += G[e] * dl;
-          const double x = __dadd_rn(Wm[e], dl);
-          const double y = __dadd_rn(Wm[et], __dmul_rn(t, Dd[et]));
-          Wt[e] = (x - y) / 2;
-        }
+          Wt[e] = __dadd_rn(Wm[e], dl);      // == skew(omega + delta) for exactly skew omega, delta
+        })
         first = block_sum(first, red);
-        // K = I + trial trial, factor test + inverse in shared memory
+        // K = I + trial trial, positive-definiteness test + inverse in shared memory
         double* Ks = smem;
-        const int kld = m + 1;
+        const int mp16 = round_up(m, 16), kld = frag_ld(mp16);
         {
           MatOp A[1] = {op_n(Wt, m)};
           MatOp B[1] = {op_n(Wt, m)};
@@ -356,12 +304,14 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           };
           eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
         }
-        const bool valid = spd_inverse_smem(Ks, m, smem + m * kld);
+        for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {   // identity padding up to mp16
+          const int i = e / mp16, j = e - i * mp16;
+          if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
+        }
+        __syncthreads();
+        const bool valid = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
         if (valid) {
-          for (int e = tid; e < mm; e += kThreads) {
-            const int i = e / m, j = e - i * m;
-            Pt[e] = Ks[i * kld + j];
-          }
+          SSN_FOR_IJ(m, { Pt[e] = Ks[i * kld + j]; })
         }
         __syncthreads();
         if (valid) {
@@ -424,10 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       auto epi = store_to(T2);
       eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
     }
-    for (int e = tid; e < mm; e += kThreads) {
-      const int i = e / m, j = e - i * m;
-      Wout[e] = (T2[e] - T2[j * m + i]) / 2;
-    }
+    SSN_FOR_IJ(m, { Wout[e] = (T2[e] - T2[j * m + i]) / 2; })
     {
       MatOp A[1] = {op_n(V, m)};
       MatOp B[2] = {op_n(Pm, m), op_n(Qm, m)};
@@ -441,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       eng.template mul<2, 1, 2, C_SHARED_B>(A, B, epi);
     }
   }
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     a.iterations[inst] = iterations;
     a.status[inst] = status;
     if (a.counters) {
@@ -454,7 +401,8 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
 }
 
 static size_t dual_smem_bytes(int MB) {
-  return sizeof(double) * (8 * (size_t)slot_doubles(MB) + 2 * kWarps + kMaxM);
+  const int region = imax(8 * slot_doubles(MB), spd_region_doubles(32 * MB));
+  return sizeof(double) * ((size_t)region + 2 * kWarps + kMaxM) + 16;
 }
 
 template <int MB>
@@ -480,14 +428,16 @@ cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
 __global__ void __launch_bounds__(kThreads, 1)
     spd_inverse_kernel(const double* K, double* P, int32_t* info, int m) {
   extern __shared__ __align__(16) double smem[];
-  const int inst = blockIdx.x, mm = m * m, ld = m + 1;
+  const int inst = blockIdx.x, mm = m * m;
+  const int mp16 = round_up(m, 16), ld = frag_ld(mp16);
+  int* flag = reinterpret_cast<int*>(smem + spd_region_doubles(m));
   const double* Kin = K + (size_t)inst * mm;
-  for (int e = threadIdx.x; e < mm; e += kThreads) {
-    const int i = e / m, j = e - i * m;
-    smem[i * ld + j] = Kin[e];
+  for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {
+    const int i = e / mp16, j = e - i * mp16;
+    smem[i * ld + j] = (i < m && j < m) ? Kin[i * m + j] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  const bool ok = spd_inverse_smem(smem, m, smem + m * ld);
+  const bool ok = spd_inverse_blocked(smem, mp16, ld, smem + mp16 * ld, flag);
   double* Pout = P + (size_t)inst * mm;
   for (int e = threadIdx.x; e < mm; e += kThreads) {
     const int i = e / m, j = e - i * m;
@@ -498,7 +448,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 cudaError_t launch_spd_inverse(const double* K, double* P, int32_t* info, int batch, int m,
                                cudaStream_t stream) {
-  const size_t smem = sizeof(double) * ((size_t)m * (m + 1) + 4 * m);
+  const size_t smem = sizeof(double) * (size_t)spd_region_doubles(m) + 16;
   cudaError_t err = cudaFuncSetAttribute(spd_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;

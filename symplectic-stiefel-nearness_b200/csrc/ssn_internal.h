@@ -32,9 +32,12 @@ struct DualArgs {
 };
 
 size_t eigh_smem_bytes(int m);
+size_t eigh_workspace_bytes(int batch, int m);
 cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, double* scale,
-                        int32_t* sweeps, int32_t* status, int batch, int m, cudaStream_t stream);
+                        int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
+                        cudaStream_t stream);
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
+cudaError_t launch_probe_fp64_mma(double* sink, int iters, double* flops, cudaStream_t stream);
 
 size_t gram_partial_doubles(int batch, int rows, int m);
 cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,

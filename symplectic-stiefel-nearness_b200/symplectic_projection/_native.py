@@ -29,9 +29,13 @@ PROTOTYPES = {
     "ssn_gram_workspace_bytes": (_SZ, [_I, _I, _I]),
     "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P]),
     "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P]),
-    "ssn_eigh": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
+    "ssn_eigh_workspace_bytes": (_SZ, [_I, _I]),
+    "ssn_eigh": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
     "ssn_dual_workspace_bytes": (_SZ, [_I, _I]),
     "ssn_dual": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
+    "ssn_newton_workspace_bytes": (_SZ, [_I, _I]),
+    "ssn_newton": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
+    "ssn_probe_fp64_mma": (_I, [_P, _I, _P, _P]),
     "ssn_inner_products": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
     "ssn_outer_skew": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
     "ssn_sandwich_front": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _P]),

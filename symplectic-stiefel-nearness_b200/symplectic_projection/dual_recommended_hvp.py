@@ -146,8 +146,11 @@ def eigh_scaled(Cr):
     vectors = torch.empty(batch, m, m, dtype=torch.float64, device=dev)
     scale = torch.empty(batch, dtype=torch.float64, device=dev)
     sweeps = torch.empty(batch, dtype=torch.int32, device=dev)
-    N.check(N.load().ssn_eigh(Cr.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(),
-                              sweeps.data_ptr(), batch, m, N.stream_handle(dev)), "ssn_eigh")
+    lib = N.load()
+    nbytes = lib.ssn_eigh_workspace_bytes(batch, m)
+    ws = workspace(dev, nbytes)
+    N.check(lib.ssn_eigh(Cr.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(),
+                         sweeps.data_ptr(), batch, m, ws.data_ptr(), nbytes, N.stream_handle(dev)), "ssn_eigh")
     return values, vectors, scale, sweeps
 
 
