@@ -305,13 +305,13 @@ def run_ours(args):
     # end to end through the public API: pinned host T -> device -> host X, omega, iterations
     e2e_ms = []
     X_host = None
-    for i in range(1 + max(1, args.e2e_steps)):
+    for i in range(2 + max(1, args.e2e_steps)):   # two untimed calls fill the pinned-buffer caches
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         X_host, W_host, I_host = sp.solve(T_host)
         e1.record(stream)
         e1.synchronize()
-        if i > 0:
+        if i > 1:
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_step = sum(e2e_ms) / max(1, len(e2e_ms))
     if world > 1:

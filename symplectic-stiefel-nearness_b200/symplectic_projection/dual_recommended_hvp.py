@@ -107,13 +107,84 @@ def solve(T: torch.Tensor, **options):
         res = solve_ex(T, **options)
         raise_for_status(res.status)
         return res.X, res.omega, res.iterations
+    return _solve_host(T, **options)
+
+
+# ---- host-resident batches: chunked, stream-pipelined staging ------------------------------
+CHUNK_BYTES = 64 * 2**20      # largest chunk of T, in bytes
+N_STREAMS = 8                 # chunks in flight; each solve is latency-bound, so they overlap
+
+_streams = {}
+_staging = {}
+
+
+def _stream_pool(dev: torch.device):
+    key = dev.index
+    if key not in _streams:
+        _streams[key] = [torch.cuda.Stream(dev) for _ in range(N_STREAMS)]
+    return _streams[key]
+
+
+def _staging_buffer(dev: torch.device, slot: int, shape) -> torch.Tensor:
+    key = (dev.index, slot)
+    numel = 1
+    for d in shape:
+        numel *= d
+    buf = _staging.get(key)
+    if buf is None or buf.numel() < numel:
+        buf = torch.empty(numel, dtype=torch.float64, pin_memory=True)
+        _staging[key] = buf
+    return buf[:numel].view(shape)
+
+
+def _solve_host(T: torch.Tensor, **options):
+    """CPU-in/CPU-out solve with the batch split into chunks on a pool of streams.
+
+    Each chunk's H2D copy, solve and D2H copy are enqueued on one stream, so
+    the copies of one chunk overlap the solves of others and the two copy
+    directions overlap each other.  A pageable T is staged through pinned
+    per-stream buffers, like the reference's pinned 1024-row staging
+    (dual_recommended_hvp.py:86-91, :204-226).
+    """
+    batch, n, m = _check_target(T)
     dev = torch.device("cuda", torch.cuda.current_device())
-    Td = T.to(dev, non_blocking=T.is_pinned())
-    res = solve_ex(Td, **options)
-    raise_for_status(res.status)
     X = _pinned_like(T)
-    X.copy_(res.X)
-    return X, res.omega.cpu(), res.iterations.cpu()
+    per = max(1, T[0].numel() * 8)
+    chunk = max(1, min(batch, CHUNK_BYTES // per, -(-batch // N_STREAMS)))
+    pinned_in, pinned_out = T.is_pinned(), X.is_pinned()
+    streams = _stream_pool(dev)
+    main = torch.cuda.current_stream(dev)
+    ready = torch.cuda.Event()
+    ready.record(main)
+    results, done = [], []
+    for idx, c0 in enumerate(range(0, batch, chunk)):
+        c1 = min(batch, c0 + chunk)
+        slot = idx % len(streams)
+        s = streams[slot]
+        s.wait_event(ready)
+        with torch.cuda.stream(s):
+            if pinned_in:
+                src = T[c0:c1]
+            else:
+                if idx >= len(streams):        # the staging buffer's previous copy must be done
+                    done[idx - len(streams)][0].synchronize()
+                src = _staging_buffer(dev, slot, (c1 - c0, 2 * n, m))
+                src.copy_(T[c0:c1])
+            Td = torch.empty((c1 - c0, 2 * n, m), dtype=torch.float64, device=dev)
+            Td.copy_(src, non_blocking=True)
+            h2d = torch.cuda.Event()
+            h2d.record(s)
+            res = solve_ex(Td, **options)
+            X[c0:c1].copy_(res.X, non_blocking=pinned_out)
+            results.append(res)
+            done.append((h2d, s))
+    for s in streams:
+        s.synchronize()
+    status = torch.cat([r.status for r in results])
+    raise_for_status(status)
+    omega = torch.cat([r.omega for r in results]).cpu()
+    iterations = torch.cat([r.iterations for r in results]).cpu()
+    return X, omega, iterations
 
 
 # ---- lower-level pieces of the reference module -------------------------------------------

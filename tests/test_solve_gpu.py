@@ -121,3 +121,17 @@ def test_batch_composition_independence(sp):
     Xb, Wb, Ib = sp.solve(T[2:5].contiguous())
     # the Gram split-K count depends on the batch size, so only rounding may differ
     assert rel(Xa[2:5], Xb) < 1e-12 and rel(Wa[2:5], Wb) < 1e-12 and torch.equal(Ia[2:5], Ib)
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_chunked_host_pipeline(sp, pinned, monkeypatch):
+    """CPU-in/CPU-out solves split into stream-pipelined chunks match the device-resident solve."""
+    from symplectic_projection import dual_recommended_hvp as D
+    T, _ = O.make_inputs(256, 24, 4, 21)
+    if pinned:
+        T = T.pin_memory()
+    monkeypatch.setattr(D, "CHUNK_BYTES", 4 * T[0].numel() * 8)   # 4 targets per chunk -> 6 chunks
+    X, W, I = sp.solve(T)
+    Xd, Wd, Id = sp.solve(T.cuda())
+    assert rel(X, Xd) < 1e-12 and rel(W, Wd) < 1e-12 and torch.equal(I, Id.cpu())
+    assert X.shape == T.shape and W.shape == (21, 48, 48)
