@@ -39,7 +39,8 @@ typedef enum {
   SSN_ERR_LINE_SEARCH = 4,      /* no descent step in MAX_BACKTRACK halvings (:190) */
   SSN_ERR_NONFINITE = 5,        /* NaN/Inf met in the input or the iteration      */
   SSN_ERR_EIGH = 6,             /* Jacobi sweeps did not converge                  */
-  SSN_ERR_WORKSPACE = 7         /* workspace missing or too small                  */
+  SSN_ERR_WORKSPACE = 7,        /* workspace missing or too small                  */
+  SSN_ERR_SCRATCH_LIMIT = 8     /* problem larger than the fixed no-allocation scratch */
 } ssn_status;
 
 /* Per-instance status words written by ssn_solve / ssn_dual (int32 per target). */
@@ -96,6 +97,23 @@ size_t ssn_gram_workspace_bytes(int batch, int rows, int m);
 int ssn_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
              int batch, int rows, int m, void* workspace, size_t workspace_bytes,
              ssn_stream_t stream);
+
+/*
+ * ssn_gram without a workspace argument, for callers that cannot allocate
+ * device memory at the call (a host framework whose pooling allocator owns the
+ * device, or a caller that must never reach cudaMalloc).  No counterpart in the
+ * reference.  Its scratch is one fixed array of ssn_gram_noalloc_scratch_bytes()
+ * (16 MiB) in the library's device memory, held by every GPU that loads the
+ * library until exit.  A call needs batch * 2 * m^2 doubles of it (more row
+ * splits are used when they fit); larger calls return SSN_ERR_SCRATCH_LIMIT
+ * without launching.  Every call shares the array: calls that overlap on the
+ * GPU race and must be serialised by the caller.  The first call on a device
+ * resolves the array's address (cudaGetSymbolAddress) and should come before
+ * any stream capture.  No call allocates.
+ */
+size_t ssn_gram_noalloc_scratch_bytes(void);
+int ssn_gram_noalloc(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
+                     int batch, int rows, int m, ssn_stream_t stream);
 
 /*
  * Recovery products:  Ur = A P^T + D Q^T,  Ui = D P^T - A Q^T.

@@ -109,6 +109,7 @@ const char* ssn_status_string(int status) {
     case SSN_ERR_NONFINITE: return "non-finite value in the iteration";
     case SSN_ERR_EIGH: return "Jacobi eigensolver did not converge";
     case SSN_ERR_WORKSPACE: return "workspace missing or too small";
+    case SSN_ERR_SCRATCH_LIMIT: return "problem exceeds the fixed scratch of the no-allocation entry point";
     default: return "unknown status";
   }
 }

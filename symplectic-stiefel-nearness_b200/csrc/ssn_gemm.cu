@@ -37,10 +37,10 @@ struct GramSplit {
   int splits, chunk;
 };
 
-static GramSplit gram_split(int batch, int rows) {
+static GramSplit gram_split(int batch, int rows, int max_splits = 1 << 30) {
   const int sms = device_sm_count();
   int want = cdiv(2 * sms, batch);
-  want = imax(1, imin(want, cdiv(rows, 64)));
+  want = imax(1, imin(imin(want, cdiv(rows, 64)), max_splits));
   int chunk = round_up(cdiv(rows, want), kPanelK);
   int splits = cdiv(rows, chunk);
   return GramSplit{splits, chunk};
@@ -105,9 +105,11 @@ __global__ void gram_finalize_kernel(const double* __restrict__ partial, double*
   }
 }
 
+int gram_splits(int batch, int rows, int max_splits) { return gram_split(batch, rows, max_splits).splits; }
+
 cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
-                        int batch, int rows, int m, double* partial, cudaStream_t stream) {
-  const GramSplit gs = gram_split(batch, rows);
+                        int batch, int rows, int m, double* partial, cudaStream_t stream, int max_splits) {
+  const GramSplit gs = gram_split(batch, rows, max_splits);
   const int MB = bucket_of(m);
   const size_t smem = sizeof(double) * 8 * (size_t)slot_doubles(MB);
   dim3 grid(gs.splits, batch);

@@ -40,8 +40,11 @@ cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
 cudaError_t launch_probe_fp64_mma(double* sink, int iters, double* flops, cudaStream_t stream);
 
 size_t gram_partial_doubles(int batch, int rows, int m);
+// number of row splits launch_gram uses for this shape when capped at max_splits
+int gram_splits(int batch, int rows, int max_splits);
 cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
-                        int batch, int rows, int m, double* partial, cudaStream_t stream);
+                        int batch, int rows, int m, double* partial, cudaStream_t stream,
+                        int max_splits = 1 << 30);
 cudaError_t launch_recover(const double* A, const double* D, int64_t ab_stride, const double* P,
                            const double* Q, double* Ur, double* Ui, int64_t u_stride, int batch,
                            int rows, int m, cudaStream_t stream);

@@ -28,6 +28,8 @@ PROTOTYPES = {
     "ssn_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_gram_workspace_bytes": (_SZ, [_I, _I, _I]),
     "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P]),
+    "ssn_gram_noalloc_scratch_bytes": (_SZ, []),
+    "ssn_gram_noalloc": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P]),
     "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P]),
     "ssn_eigh_workspace_bytes": (_SZ, [_I, _I]),
     "ssn_eigh": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
@@ -49,7 +51,7 @@ PROTOTYPES = {
 
 SSN_OK = 0
 STATUS_NAMES = {0: "converged", 1: "invalid argument", 2: "CUDA error", 3: "Newton cap",
-                4: "line search", 5: "non-finite", 6: "eigh", 7: "workspace"}
+                4: "line search", 5: "non-finite", 6: "eigh", 7: "workspace", 8: "scratch limit"}
 
 
 class Options(ctypes.Structure):
