@@ -349,9 +349,9 @@ __device__ __forceinline__ void smem_product(int R, int N, int K, const double* 
 // they are all positive exactly when K is positive definite (the test
 // torch.linalg.cholesky_ex applies).  K: mp x mp (mp = m rounded up to 16;
 // the caller pads the tail with the identity), leading dim ld == 4 (mod 16).
-// scratch: 16 * ld + mp * 20 doubles.  Returns the same bool in every thread.
+// scratch: 16 * ld + 2 * mp * 20 doubles.  Returns the same bool in every thread.
 __host__ __device__ constexpr int spd_region_doubles(int m) {
-  return round_up(m, 16) * frag_ld(round_up(m, 16)) + 16 * frag_ld(round_up(m, 16)) + round_up(m, 16) * 20;
+  return round_up(m, 16) * frag_ld(round_up(m, 16)) + 16 * frag_ld(round_up(m, 16)) + 2 * round_up(m, 16) * 20;
 }
 
 __device__ __forceinline__ bool spd_inverse_blocked(double* K, int mp, int ld, double* scratch,
@@ -359,59 +359,64 @@ __device__ __forceinline__ bool spd_inverse_blocked(double* K, int mp, int ld, d
   constexpr int b = 16;
   double* U = scratch;               // b x ld   : U[p][j]
   double* W = scratch + b * ld;      // mp x b   stored as W[j][p] with leading dim 20
+  double* X = W + mp * 20;           // mp x b   old K_:,P, leading dim 20
   if (threadIdx.x == 0) *flag = 1;
   for (int k0 = 0; k0 < mp; k0 += b) {
-    // (1) warp 0 inverts the b x b diagonal block in place (scalar sweep operator)
+    // (1) warp 0 inverts the b x b diagonal block (scalar sweep operator) in
+    // registers: lane (i, h) = (lane & 15, lane >> 4) holds row i, columns
+    // 8h .. 8h+7; the pivot row, a_ik and the pivot are broadcast by shuffles,
+    // so the sequential pivot chain never goes through shared memory.
     if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
+      const int lane = threadIdx.x, i = lane & 15, h = lane >> 4;
+      double r[8];
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) r[jj] = K[(k0 + i) * ld + k0 + 8 * h + jj];
       bool ok = true;
+#pragma unroll
       for (int k = 0; k < b; ++k) {
-        __syncwarp();
-        const double piv = K[(k0 + k) * ld + k0 + k];
-        if (!(piv > 0.0) || !isfinite(piv)) { ok = false; break; }
-        const double inv = 1.0 / piv;
-        // each lane owns row i = lane & 15, columns j = (lane >> 4) * 8 + 0..7
-        const int i = lane & 15, jb = (lane >> 4) * 8;
-        const double aik = K[(k0 + i) * ld + k0 + k];
+        const int hk = k >> 3, ck = k & 7;              // column k lives in half hk, slot ck
+        const double piv = __shfl_sync(0xffffffffu, r[ck], k + 16 * hk);
+        const double aik = __shfl_sync(0xffffffffu, r[ck], i + 16 * hk);
         double rowk[8];
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) rowk[jj] = K[(k0 + k) * ld + k0 + jb + jj];
-        __syncwarp();
+        for (int jj = 0; jj < 8; ++jj) rowk[jj] = __shfl_sync(0xffffffffu, r[jj], k + 16 * h);
+        ok = ok && (piv > 0.0) && isfinite(piv);
+        const double inv = 1.0 / piv;
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
-          const int j = jb + jj;
+          const bool col_k = (h == hk) && (jj == ck);
           double v;
-          if (i == k) v = (j == k) ? inv : rowk[jj] * inv;
-          else if (j == k) v = -aik * inv;
-          else v = K[(k0 + i) * ld + k0 + j] - aik * (rowk[jj] * inv);
-          K[(k0 + i) * ld + k0 + j] = v;
+          if (i == k) v = col_k ? inv : rowk[jj] * inv;
+          else if (col_k) v = -aik * inv;
+          else v = r[jj] - aik * (rowk[jj] * inv);
+          r[jj] = v;
         }
       }
-      __syncwarp();
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) K[(k0 + i) * ld + k0 + 8 * h + jj] = r[jj];
       if (lane == 0 && !ok) *flag = 0;
     }
     __syncthreads();
     if (*flag == 0) return false;
-    // (2) U = Dinv K_P,:  and  W = K_:,P Dinv  (P columns/rows skipped later)
+    // (2) U = Dinv K_P,:, W = K_:,P Dinv, and a copy X = K_:,P (old) for the update
     const double* Dinv = K + k0 * ld + k0;
     smem_product<false, false>(b, mp, b, Dinv, ld, K + k0 * ld, ld,
                                [&](int p, int j, double v) { U[p * ld + j] = v; });
     smem_product<false, false>(mp, b, b, K + k0, ld, Dinv, ld,
                                [&](int j, int p, double v) { W[j * 20 + p] = v; });
+    for (int j = threadIdx.x >> 4; j < mp; j += blockDim.x >> 4) X[j * 20 + (threadIdx.x & 15)] = K[j * ld + k0 + (threadIdx.x & 15)];
     __syncthreads();
-    // (3) K_QQ -= K_QP U   (rows/cols of P are rewritten in (4))
-    smem_product<false, false>(mp, mp, b, K + k0, ld, U, ld, [&](int i, int j, double v) {
-      const bool in_p = (i >= k0 && i < k0 + b) || (j >= k0 && j < k0 + b);
-      if (!in_p) K[i * ld + j] -= v;
+    // (3) K_QQ -= X U, K_PQ = U, K_QP = -W  (disjoint entries, one phase)
+    smem_product<false, false>(mp, mp, b, X, 20, U, ld, [&](int i, int j, double v) {
+      const bool ip = i >= k0 && i < k0 + b, jp = j >= k0 && j < k0 + b;
+      if (!ip && !jp) K[i * ld + j] -= v;
     });
-    __syncthreads();
-    // (4) K_PQ = U, K_QP = -W
-    for (int e = threadIdx.x; e < b * mp; e += blockDim.x) {
-      const int p = e / mp, j = e - p * mp;
-      if (j >= k0 && j < k0 + b) continue;
-      K[(k0 + p) * ld + j] = U[p * ld + j];
-      K[j * ld + k0 + p] = -W[j * 20 + p];
-    }
+    for (int p = threadIdx.x >> 5; p < b; p += blockDim.x >> 5)
+      for (int j = threadIdx.x & 31; j < mp; j += 32) {
+        if (j >= k0 && j < k0 + b) continue;
+        K[(k0 + p) * ld + j] = U[p * ld + j];
+        K[j * ld + k0 + p] = -W[j * 20 + p];
+      }
     __syncthreads();
   }
   return true;

@@ -7,11 +7,11 @@
 // if |a_pq| > eps * sqrt(|a_pp a_qq|); a sweep without rotations ends it.
 //
 // Two kernels:
-//  * values (one CTA per instance, A in shared memory), two phases per step:
-//    m/2 threads compute the step's rotations and its pair table; then every
-//    2 x 2 block (pair a rows) x (pair b columns) is updated independently as
-//    A' = J_a^T A J_b.  Each applied step's (c, s) is appended to a rotation
-//    log in the workspace.
+//  * values (one CTA per instance, A in shared memory), one barrier per step:
+//    every 2 x 2 block (pair a rows) x (pair b columns) is updated independently
+//    as A' = J_a^T A J_b; the threads owning the fixed "host" blocks (which hold
+//    the next step's pairs) also compute the next step's rotations.  Each
+//    applied step's (c, s) is appended to a rotation log in the workspace.
 //  * vectors (one warp per row of V): rows of V = J_1 J_2 ... are independent
 //    under column rotations, so each warp replays the log on its own row with
 //    warp-level synchronisation only, spread over all SMs.
@@ -56,6 +56,28 @@ size_t eigh_log_doubles(int batch, int m) {
   return (size_t)batch * kMaxSweeps * (m - 1) * M * 2;
 }
 
+// Circle method in slot space: after one step the index in slot u (u >= 1)
+// moves to slot u - 1 (slot 1 wraps to slot m - 1); slot 0 is fixed.  Hence the
+// pair a' of the next step is formed by the step-st slots (a' + 1, m - a')
+// (a' >= 1) or (0, 1) (a' = 0): one entry of the 2 x 2 block of the current
+// slot pairs (a' - 1, min(a' + 1, m - 2 - a')) or (0, 1).  That "host" block
+// is the same for every step, so a fixed set of threads can update it and
+// compute the next rotation right away, without a second barrier.
+__device__ __forceinline__ int pair_of_slot(int u, int m) { return u < m - 1 - u ? u : m - 1 - u; }
+
+__device__ __forceinline__ void host_block(int ap, int m, int& bx, int& by, int& sx, int& sy) {
+  // next-step pair ap lives at step-st slots (sx, sy) inside slot-pair block (bx, by)
+  if (ap == 0) {
+    sx = 0;
+    sy = 1;
+  } else {
+    sx = m - ap;
+    sy = ap + 1;
+  }
+  bx = pair_of_slot(sx, m);
+  by = pair_of_slot(sy, m);
+}
+
 __global__ void __launch_bounds__(kJacobiThreads, 1)
     jacobi_values_kernel(const double* __restrict__ Cr, double* __restrict__ values,
                          double* __restrict__ scale_out, int32_t* __restrict__ sweeps_out,
@@ -65,13 +87,18 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   const int inst = blockIdx.x, tid = threadIdx.x;
   const int ld = m + 1, M = m / 2, m1 = m - 1;
   double* A = sm;                                                    // m x ld
-  double2* cs = reinterpret_cast<double2*>(A + ((m * ld + 1) & ~1)); // [64]: (c, s) of the current step
-  double* tt = reinterpret_cast<double*>(cs + 64);                   // [64]: tan of the current step
-  int2* pq = reinterpret_cast<int2*>(tt + 64);                       // [64]: (p, q) of the current step, p < q
-  double* red = reinterpret_cast<double*>(pq + 64);                  // kJacobiThreads/32
+  double2* cs = reinterpret_cast<double2*>(A + ((m * ld + 1) & ~1)); // [2][64]: (c, s)
+  double2* dg = cs + 2 * 64;                                         // [2][64]: diagonal entries after the rotation
+  double* tt = reinterpret_cast<double*>(dg + 2 * 64);               // [2][64]: tan
+  int2* pq = reinterpret_cast<int2*>(tt + 2 * 64);                   // [2][64]: (p, q), p < q
+  double* red = reinterpret_cast<double*>(pq + 2 * 64);              // kJacobiThreads/32
   int* ctl = reinterpret_cast<int*>(red + kJacobiThreads / 32);      // [0..1]: rotated in sweep (parity), [2]: last step+1
-  short2* blk = reinterpret_cast<short2*>(ctl + 4);                  // off-diagonal blocks a < b
-  const int nblk = M * (M - 1) / 2;
+  short2* blk = reinterpret_cast<short2*>(ctl + 4);                  // blocks of the generic threads
+  // m >= 6: warps 0-1 own the M host blocks; the other warps own the rest (incl. diagonal blocks).
+  // m <= 4: host blocks coincide, so rotations are computed in a separate phase instead.
+  const bool hosted = m >= 6;
+  constexpr int kHostThreads = 64;
+  constexpr int kHostFlag = 0x100;
 
   const double* C = Cr + (size_t)inst * m * m;
   double* L = rlog + (size_t)inst * kMaxSweeps * m1 * M * 2;
@@ -83,71 +110,158 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
     const int i = e / m, j = e - i * m;
     A[i * ld + j] = C[e] / scale;
   }
+  // block list: off-diagonal blocks (a < b) row-major, then the diagonal blocks.
+  // Host blocks carry kHostFlag in .y and are skipped by the generic threads.
+  // Block (a, b), a < b, hosts next pair a' iff it equals (a' - 1, P1(a')) with
+  // P1(a') = min(a' + 1, m - 2 - a'), or is (0, 1) (a' = 0): an O(1) test.
+  const int noff = M * (M - 1) / 2, nblk = noff + M;
   for (int k = tid; k < nblk; k += kJacobiThreads) {
-    int a = 0, r = k;   // row-major strict upper triangle: row a holds M - 1 - a blocks
-    while (r >= M - 1 - a) { r -= M - 1 - a; ++a; }
-    blk[k] = make_short2((short)a, (short)(a + 1 + r));
+    int a, b;
+    if (k < noff) {
+      a = 0;
+      int r = k;
+      while (r >= M - 1 - a) { r -= M - 1 - a; ++a; }
+      b = a + 1 + r;
+    } else {
+      a = b = k - noff;
+    }
+    bool host = false;
+    if (hosted && a != b) {
+      auto p1 = [&](int ap) { return imin(ap + 1, m - 2 - ap); };
+      host = (a == 0 && b == 1) || (a + 1 < M && p1(a + 1) == b) || (b + 1 < M && p1(b + 1) == a);
+    }
+    blk[k] = make_short2((short)a, (short)(host ? (b | kHostFlag) : b));
   }
   if (tid == 0) { ctl[0] = 0; ctl[1] = 0; ctl[2] = 0; ctl[3] = 0; }
+  __syncthreads();
+
+  auto rotate_pair = [&](int a, int st, int buf, int g, double app, double aqq, double apq, int p, int q) {
+    double c, s, t;
+    const bool rot = make_rotation(app, aqq, apq, c, s, t);
+    cs[buf * 64 + a] = make_double2(c, s);
+    dg[buf * 64 + a] = make_double2(app - t * apq, aqq + t * apq);
+    tt[buf * 64 + a] = t;
+    pq[buf * 64 + a] = make_int2(p, q);
+    L[((size_t)g * M + a) * 2 + 0] = c;
+    L[((size_t)g * M + a) * 2 + 1] = s;
+    return rot;
+  };
+
+  // rotations of step 0
+  if (tid < M) {
+    int p = rr_index(tid, 0, m1), q = rr_index(m - 1 - tid, 0, m1);
+    if (p > q) { const int x = p; p = q; q = x; }
+    if (rotate_pair(tid, 0, 0, 0, A[p * ld + p], A[q * ld + q], A[p * ld + q], p, q)) {
+      ctl[0] = 1;
+      ctl[2] = 1;
+    }
+  }
   __syncthreads();
 
   int g = 0, st = 0, sweep = 0;
   bool converged = false;
   const int max_steps = kMaxSweeps * m1;
   while (g < max_steps) {
-    // phase 1: rotations of this step (M threads), logged for the vectors kernel
-    if (tid < M) {
-      int p = rr_index(tid, st, m1), q = rr_index(m - 1 - tid, st, m1);
-      if (p > q) { const int x = p; p = q; q = x; }
-      double c, s, t;
-      const bool rot = make_rotation(A[p * ld + p], A[q * ld + q], A[p * ld + q], c, s, t);
-      cs[tid] = make_double2(c, s);
-      tt[tid] = t;
-      pq[tid] = make_int2(p, q);
-      L[((size_t)g * M + tid) * 2 + 0] = c;
-      L[((size_t)g * M + tid) * 2 + 1] = s;
-      if (rot) { ctl[sweep & 1] = 1; ctl[2] = g + 1; }
-    }
-    __syncthreads();
-    // phase 2: A <- J^T A J, every 2 x 2 block (pair a rows) x (pair b columns) independently
-    for (int k = tid; k < nblk + M; k += kJacobiThreads) {
-      if (k >= nblk) {                 // diagonal block of pair a
-        const int a = k - nblk;
-        const double2 r = cs[a];
-        if (r.y == 0.0) continue;
-        const int2 ia = pq[a];
-        const double t = tt[a], apq = A[ia.x * ld + ia.y];
-        A[ia.x * ld + ia.x] -= t * apq;
-        A[ia.y * ld + ia.y] += t * apq;
-        A[ia.x * ld + ia.y] = 0.0;
-        A[ia.y * ld + ia.x] = 0.0;
-        continue;
+    const int cur = g & 1, nxt = cur ^ 1;
+    const int nsweep = (st + 1 == m1) ? sweep + 1 : sweep;
+    const double2* csc = cs + cur * 64;
+    const double2* dgc = dg + cur * 64;
+    const int2* pqc = pq + cur * 64;
+    if (hosted && tid < kHostThreads) {
+      const int ap = tid;
+      if (ap < M && g + 1 < max_steps) {
+        int bx, by, sx, sy;
+        host_block(ap, m, bx, by, sx, sy);
+        const int x = rr_index(sx, st, m1), y = rr_index(sy, st, m1);   // next pair's indices
+        const double2 ra = csc[bx], rb = csc[by];
+        const int2 ia = pqc[bx], ib = pqc[by];
+        double nv[2][2];
+        nv[0][0] = A[ia.x * ld + ib.x];
+        nv[0][1] = A[ia.x * ld + ib.y];
+        nv[1][0] = A[ia.y * ld + ib.x];
+        nv[1][1] = A[ia.y * ld + ib.y];
+        if (ra.y != 0.0 || rb.y != 0.0) {
+          const double u0 = ra.x * nv[0][0] - ra.y * nv[1][0], u1 = ra.x * nv[0][1] - ra.y * nv[1][1];
+          const double v0 = ra.y * nv[0][0] + ra.x * nv[1][0], v1 = ra.y * nv[0][1] + ra.x * nv[1][1];
+          nv[0][0] = u0 * rb.x - u1 * rb.y;
+          nv[0][1] = u0 * rb.y + u1 * rb.x;
+          nv[1][0] = v0 * rb.x - v1 * rb.y;
+          nv[1][1] = v0 * rb.y + v1 * rb.x;
+          A[ia.x * ld + ib.x] = nv[0][0];
+          A[ib.x * ld + ia.x] = nv[0][0];
+          A[ia.x * ld + ib.y] = nv[0][1];
+          A[ib.y * ld + ia.x] = nv[0][1];
+          A[ia.y * ld + ib.x] = nv[1][0];
+          A[ib.x * ld + ia.y] = nv[1][0];
+          A[ia.y * ld + ib.y] = nv[1][1];
+          A[ib.y * ld + ia.y] = nv[1][1];
+        }
+        // x belongs to pair bx, y to pair by; their diagonal entries after this step
+        const int ux = (x == ia.x) ? 0 : 1, uy = (y == ib.x) ? 0 : 1;
+        const double dx = ux == 0 ? dgc[bx].x : dgc[bx].y;
+        const double dy = uy == 0 ? dgc[by].x : dgc[by].y;
+        const double axy = nv[ux][uy];
+        const bool xfirst = x < y;
+        if (rotate_pair(ap, 0, nxt, g + 1, xfirst ? dx : dy, xfirst ? dy : dx, axy, xfirst ? x : y,
+                        xfirst ? y : x)) {
+          ctl[nsweep & 1] = 1;
+          ctl[2] = g + 2;
+        }
       }
-      const short2 ab = blk[k];
-      const double2 ra = cs[ab.x], rb = cs[ab.y];
-      if (ra.y == 0.0 && rb.y == 0.0) continue;
-      const int2 ia = pq[ab.x], ib = pq[ab.y];
-      const double x = A[ia.x * ld + ib.x], y = A[ia.x * ld + ib.y];
-      const double z = A[ia.y * ld + ib.x], w = A[ia.y * ld + ib.y];
-      const double u0 = ra.x * x - ra.y * z, u1 = ra.x * y - ra.y * w;   // rows of J_a^T M
-      const double v0 = ra.y * x + ra.x * z, v1 = ra.y * y + ra.x * w;
-      const double n00 = u0 * rb.x - u1 * rb.y, n01 = u0 * rb.y + u1 * rb.x;
-      const double n10 = v0 * rb.x - v1 * rb.y, n11 = v0 * rb.y + v1 * rb.x;
-      A[ia.x * ld + ib.x] = n00;
-      A[ib.x * ld + ia.x] = n00;
-      A[ia.x * ld + ib.y] = n01;
-      A[ib.y * ld + ia.x] = n01;
-      A[ia.y * ld + ib.x] = n10;
-      A[ib.x * ld + ia.y] = n10;
-      A[ia.y * ld + ib.y] = n11;
-      A[ib.y * ld + ia.y] = n11;
+    } else if (hosted || tid >= 0) {
+      const int first = hosted ? tid - kHostThreads : tid;
+      const int stride = hosted ? kJacobiThreads - kHostThreads : kJacobiThreads;
+      for (int k = first; k < nblk; k += stride) {
+        const short2 ab = blk[k];
+        if (ab.y & kHostFlag) continue;          // owned by a host thread
+        const double2 ra = csc[ab.x];
+        if (ab.x == ab.y) {                      // diagonal block of pair a
+          if (ra.y == 0.0) continue;
+          const int2 ia = pqc[ab.x];
+          const double2 d = dgc[ab.x];
+          A[ia.x * ld + ia.x] = d.x;
+          A[ia.y * ld + ia.y] = d.y;
+          A[ia.x * ld + ia.y] = 0.0;
+          A[ia.y * ld + ia.x] = 0.0;
+          continue;
+        }
+        const double2 rb = csc[ab.y];
+        if (ra.y == 0.0 && rb.y == 0.0) continue;
+        const int2 ia = pqc[ab.x], ib = pqc[ab.y];
+        const double x = A[ia.x * ld + ib.x], y = A[ia.x * ld + ib.y];
+        const double z = A[ia.y * ld + ib.x], w = A[ia.y * ld + ib.y];
+        const double u0 = ra.x * x - ra.y * z, u1 = ra.x * y - ra.y * w;   // rows of J_a^T M
+        const double v0 = ra.y * x + ra.x * z, v1 = ra.y * y + ra.x * w;
+        const double n00 = u0 * rb.x - u1 * rb.y, n01 = u0 * rb.y + u1 * rb.x;
+        const double n10 = v0 * rb.x - v1 * rb.y, n11 = v0 * rb.y + v1 * rb.x;
+        A[ia.x * ld + ib.x] = n00;
+        A[ib.x * ld + ia.x] = n00;
+        A[ia.x * ld + ib.y] = n01;
+        A[ib.y * ld + ia.x] = n01;
+        A[ia.y * ld + ib.x] = n10;
+        A[ib.x * ld + ia.y] = n10;
+        A[ia.y * ld + ib.y] = n11;
+        A[ib.y * ld + ia.y] = n11;
+      }
     }
     __syncthreads();
+    if (!hosted && g + 1 < max_steps) {     // m <= 4: rotations of the next step in their own phase
+      const int nst = (st + 1 == m1) ? 0 : st + 1;
+      if (tid < M) {
+        int p = rr_index(tid, nst, m1), q = rr_index(m - 1 - tid, nst, m1);
+        if (p > q) { const int x = p; p = q; q = x; }
+        if (rotate_pair(tid, nst, nxt, g + 1, A[p * ld + p], A[q * ld + q], A[p * ld + q], p, q)) {
+          ctl[nsweep & 1] = 1;
+          ctl[2] = g + 2;
+        }
+      }
+      __syncthreads();
+    }
     ++g;
     if (++st == m1) {  // a sweep ended: stop after a sweep without rotations
       st = 0;
-      // flags of this sweep's parity were last written before the barrier above;
-      // the next writer of this slot is two sweeps away, behind many barriers
+      // this sweep's flag was last written before the barrier above; the next
+      // writer of this parity slot is two sweeps away, behind many barriers
       const bool any = ctl[sweep & 1] != 0;
       __syncthreads();
       if (tid == 0) ctl[sweep & 1] = 0;
@@ -181,12 +295,13 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   }
 }
 
-constexpr int kVecWarps = 8;
-constexpr int kVecChunk = 32;   // log steps staged in shared memory at a time
+constexpr int kVecWarps = 16;
+constexpr int kVecChunk = 16;   // log steps staged in shared memory at a time
 
-// V = J_1 J_2 ... J_n applied to the identity, one warp per row of V; the CTA
-// stages the rotation log through shared memory in chunks of kVecChunk steps.
-// Columns are written in ascending eigenvalue order.
+// V = J_1 J_2 ... J_n applied to the identity, one warp per row of V.  The CTA
+// keeps the pair table of all m - 1 steps of a sweep and stages the rotation
+// log through shared memory in chunks of kVecChunk steps.  Columns are written
+// in ascending eigenvalue order.
 __global__ void __launch_bounds__(kVecWarps * 32)
     jacobi_vectors_kernel(const double* __restrict__ rlog, const int32_t* __restrict__ nsteps,
                           const int32_t* __restrict__ order, double* __restrict__ vectors, int m) {
@@ -196,6 +311,13 @@ __global__ void __launch_bounds__(kVecWarps * 32)
   const int M = m / 2, m1 = m - 1, ld = m + 1;
   double2* chunk = reinterpret_cast<double2*>(sv);                    // [kVecChunk][M]
   double* v = sv + 2 * kVecChunk * M + warp * ld;
+  short2* pt = reinterpret_cast<short2*>(sv + 2 * kVecChunk * M + kVecWarps * ld);  // [m1][M]
+  for (int e = threadIdx.x; e < m1 * M; e += kVecWarps * 32) {
+    const int st = e / M, a = e - st * M;
+    int p = rr_index(a, st, m1), q = rr_index(m - 1 - a, st, m1);
+    if (p > q) { const int x = p; p = q; q = x; }
+    pt[e] = make_short2((short)p, (short)q);
+  }
   const bool active = row < m;
   if (active)
     for (int c = lane; c < m; c += 32) v[c] = (c == row) ? 1.0 : 0.0;
@@ -209,20 +331,19 @@ __global__ void __launch_bounds__(kVecWarps * 32)
     __syncthreads();
     if (active) {
       for (int gg = 0; gg < cnt; ++gg) {
+        const double2* cr = chunk + gg * M;
+        const short2* pr = pt + st * M;
         for (int a = lane; a < M; a += 32) {
-          const double2 r = chunk[gg * M + a];
+          const double2 r = cr[a];
           if (r.y == 0.0) continue;
-          int p = rr_index(a, st, m1), q = rr_index(m - 1 - a, st, m1);
-          if (p > q) { const int x = p; p = q; q = x; }
-          const double vp = v[p], vq = v[q];
-          v[p] = r.x * vp - r.y * vq;
-          v[q] = r.y * vp + r.x * vq;
+          const short2 ij = pr[a];
+          const double vp = v[ij.x], vq = v[ij.y];
+          v[ij.x] = r.x * vp - r.y * vq;
+          v[ij.y] = r.y * vp + r.x * vq;
         }
         __syncwarp();
         st = (st + 1 == m1) ? 0 : st + 1;
       }
-    } else {
-      st = (st + cnt) % m1;
     }
   }
   if (!active) return;
@@ -233,9 +354,9 @@ __global__ void __launch_bounds__(kVecWarps * 32)
 
 size_t eigh_smem_bytes(int m) {
   const int M = m / 2;
-  return sizeof(double) * ((size_t)((m * (m + 1) + 1) & ~1)) + sizeof(double2) * 64 + sizeof(double) * 64 +
-         sizeof(int2) * 64 + sizeof(double) * (kJacobiThreads / 32) + sizeof(int) * 4 +
-         sizeof(short2) * (size_t)(M * (M - 1) / 2 + 1) + 16;
+  return sizeof(double) * ((size_t)((m * (m + 1) + 1) & ~1)) + sizeof(double2) * 4 * 64 +
+         sizeof(double) * 2 * 64 + sizeof(int2) * 2 * 64 + sizeof(double) * (kJacobiThreads / 32) +
+         sizeof(int) * 4 + sizeof(short2) * (size_t)(M * (M + 1) / 2 + 1) + 16;
 }
 
 size_t eigh_workspace_bytes(int batch, int m) {
@@ -256,7 +377,11 @@ cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, doubl
                                                                nsteps, order, m);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
-  const size_t vsmem = sizeof(double) * (2 * kVecChunk * (m / 2) + kVecWarps * (m + 1));
+  const size_t vsmem = sizeof(double) * (2 * kVecChunk * (m / 2) + kVecWarps * (m + 1)) +
+                       sizeof(short2) * (size_t)(m - 1) * (m / 2) + 16;
+  err = cudaFuncSetAttribute(jacobi_vectors_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(vsmem));
+  if (err != cudaSuccess) return err;
   dim3 grid(cdiv(m, kVecWarps), batch);
   jacobi_vectors_kernel<<<grid, kVecWarps * 32, vsmem, stream>>>(rlog, nsteps, order, vectors, m);
   return cudaGetLastError();

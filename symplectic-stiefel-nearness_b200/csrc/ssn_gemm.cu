@@ -39,7 +39,7 @@ struct GramSplit {
 
 static GramSplit gram_split(int batch, int rows, int max_splits = 1 << 30) {
   const int sms = device_sm_count();
-  int want = cdiv(2 * sms, batch);
+  int want = imin(cdiv(2 * sms, batch), 16);
   want = imax(1, imin(imin(want, cdiv(rows, 64)), max_splits));
   int chunk = round_up(cdiv(rows, want), kPanelK);
   int splits = cdiv(rows, chunk);
@@ -81,28 +81,30 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// One thread per upper-triangle entry (i <= j) of every instance: sums the
+// row-split partials in split order, mirrors Cr and forms Ci = G - G^T.
 __global__ void gram_finalize_kernel(const double* __restrict__ partial, double* __restrict__ Cr,
                                      double* __restrict__ Ci, int m, int splits) {
-  const int b = blockIdx.x, mm = m * m;
+  const int b = blockIdx.y, mm = m * m;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= mm) return;
+  const int i = e / m, j = e - i * m;
+  if (i > j) return;
   const double* p = partial + (size_t)b * splits * 2 * mm;
+  double sr = 0.0, gij = 0.0, gji = 0.0;
+  for (int s = 0; s < splits; ++s) {
+    const double* q = p + (size_t)s * 2 * mm;
+    sr += q[e];
+    gij += q[mm + e];
+    gji += q[mm + j * m + i];
+  }
   double* cr = Cr + (size_t)b * mm;
   double* ci = Ci + (size_t)b * mm;
-  for (int e = threadIdx.x; e < mm; e += blockDim.x) {
-    const int i = e / m, j = e - i * m;
-    if (i > j) continue;
-    double sr = 0.0, gij = 0.0, gji = 0.0;
-    for (int s = 0; s < splits; ++s) {
-      const double* q = p + (size_t)s * 2 * mm;
-      sr += q[e];
-      gij += q[mm + e];
-      gji += q[mm + j * m + i];
-    }
-    cr[e] = sr;
-    cr[j * m + i] = sr;
-    const double c = gij - gji;
-    ci[e] = c;
-    ci[j * m + i] = -c;
-  }
+  cr[e] = sr;
+  cr[j * m + i] = sr;
+  const double c = gij - gji;
+  ci[e] = c;
+  ci[j * m + i] = -c;
 }
 
 int gram_splits(int batch, int rows, int max_splits) { return gram_split(batch, rows, max_splits).splits; }
@@ -131,7 +133,7 @@ cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, dou
 #undef SSN_GRAM_CASE
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
-  gram_finalize_kernel<<<batch, 256, 0, stream>>>(partial, Cr, Ci, m, gs.splits);
+  gram_finalize_kernel<<<dim3(cdiv(m * m, 128), batch), 128, 0, stream>>>(partial, Cr, Ci, m, gs.splits);
   return cudaGetLastError();
 }
 
