@@ -19,8 +19,12 @@
 #include <float.h>
 #include <math.h>
 
+#include <cooperative_groups.h>
+
 #include "ssn_common.cuh"
 #include "ssn_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace ssn {
 
@@ -37,42 +41,128 @@ constexpr uint32_t C_DIFF = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 2);
 constexpr uint32_t C_CPLX = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1) | coef_bit(1, 1, 0, 1) |
                             coef_bit(1, 0, 1, 2);
 
-template <int MB>
-struct Dual {
-  int m, mm;
-  double* smem;
-  int slot;
+// Warp-tile shape of a CL-way row split for bucket MB: each CTA computes at most
+// round_up(32*MB / CL, 8) rows of every m x m product.
+template <int MB, int CL, int NOUT>
+struct SplitTile {
+  static constexpr int WC = MB;
+  static constexpr int WR = CL == 1 ? Tile<MB, NOUT>::WR : imax(1, cdiv(16 * MB, 32));
+};
 
-  template <int NA, int NB, int NOUT, uint32_t COEF, class Epi>
-  __device__ __forceinline__ void mul(const MatOp (&A)[NA], const MatOp (&B)[NB], Epi& epi) const {
-    using TL = Tile<MB, NOUT>;
-    ssn::tile_product<TL::WR, TL::WC, NA, NB, NOUT, COEF>(A, B, m, m, m, smem, slot, epi);
+// The CTAs that work on one instance: CL = 1 (one CTA) or CL = 2 (a thread-block
+// cluster splitting every m x m product and pass by rows).  sync() is the phase
+// barrier; sum() is a CTA reduction followed, for CL = 2, by a fixed-order sum of
+// the two CTA partials exchanged through distributed shared memory, so both
+// CTAs obtain identical bits and branch identically.
+template <int CL>
+struct Team {
+  int rank, r0, r1;       // rows [r0, r1) of every m x m matrix belong to this CTA
+  double* red;            // 2*kWarps doubles (CTA reduction)
+  double* xch;            // [2 parities][2 values][CL ranks] exchange slots (local)
+  double* xch_peer;       // the same slots in the peer CTA (CL = 2)
+  int parity;
+
+  __device__ __forceinline__ void sync() {
+    if constexpr (CL == 1) {
+      __syncthreads();
+    } else {
+      cg::this_cluster().sync();
+    }
+  }
+  __device__ __forceinline__ void sum2(double& a, double& b) {
+    block_sum2(a, b, red);
+    if constexpr (CL == 2) {
+      double* slot = xch + parity * 4;
+      double* peer = xch_peer + parity * 4;
+      if (threadIdx.x == 0) {
+        slot[rank] = a;
+        slot[2 + rank] = b;
+        peer[rank] = a;
+        peer[2 + rank] = b;
+      }
+      cg::this_cluster().sync();
+      a = slot[0] + slot[1];
+      b = slot[2] + slot[3];
+      parity ^= 1;
+    }
+  }
+  __device__ __forceinline__ double sum(double a) {
+    double b = 0.0;
+    sum2(a, b);
+    return a;
   }
 };
 
-// Element loops without integer division: warp w owns rows w, w+16, ..., lane l
-// owns columns l, l+32, ...; consecutive lanes touch consecutive addresses.
-#define SSN_FOR_IJ(m_, BODY)                                                          \
-  for (int i = (int)(threadIdx.x >> 5); i < (m_); i += kWarps)                        \
+template <int MB, int CL>
+struct Dual {
+  int m;
+  double* smem;
+  int slot;
+  int r0, rows;
+
+  // rows [r0, r0 + rows) of sum_{a,b} +-op(A_a) op(B_b); epi gets global row indices
+  template <int NA, int NB, int NOUT, uint32_t COEF, class Epi>
+  __device__ __forceinline__ void mul(const MatOp (&A)[NA], const MatOp (&B)[NB], Epi& epi) const {
+    using TL = SplitTile<MB, CL, NOUT>;
+    MatOp As[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      As[a] = A[a];
+      As[a].ptr = A[a].trans ? A[a].ptr + r0 : A[a].ptr + (size_t)r0 * A[a].ld;
+    }
+    const int off = r0;
+    auto shifted = [&](int o, int i, int j, double v) { epi(o, i + off, j, v); };
+    ssn::tile_product<TL::WR, TL::WC, NA, NB, NOUT, COEF>(As, B, rows, m, m, smem, slot, shifted);
+  }
+};
+
+// Element loops over this CTA's rows without integer division: warp w owns rows
+// r0 + w, r0 + w + 16, ..., lane l owns columns l, l+32, ...
+#define SSN_FOR_IJ(T_, m_, BODY)                                                      \
+  for (int i = (T_).r0 + (int)(threadIdx.x >> 5); i < (T_).r1; i += kWarps)          \
     for (int j = (int)(threadIdx.x & 31); j < (m_); j += 32) {                        \
       const int e = i * (m_) + j;                                                     \
       (void)e;                                                                        \
       BODY                                                                            \
     }
 
-template <int MB>
+template <int MB, int CL>
 __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   extern __shared__ __align__(16) double smem[];
-  const int inst = blockIdx.x;
   const int m = a.m, mm = m * m;
+  const int rank = CL == 1 ? 0 : (int)cg::this_cluster().block_rank();
+  const int inst = blockIdx.x / CL;
   const int slot = slot_doubles(MB);
   const int region = imax(8 * slot, spd_region_doubles(m));
   double* red = smem + region;                // 2*kWarps doubles
-  double* lam = red + 2 * kWarps;             // m doubles
-  int* flag = reinterpret_cast<int*>(lam + kMaxM);
-  double* Zs = smem;                          // m x (m+1): HVP outer product, after the engine
+  double* lam = red + 2 * kWarps;             // kMaxM doubles
+  double* xch = lam + kMaxM;                  // 8 doubles
+  int* flag = reinterpret_cast<int*>(xch + 8);
+  double* Zs = smem;                          // this CTA's rows of the HVP outer product
   const int zld = m + 1;
-  Dual<MB> eng{m, mm, smem, slot};
+
+  const int half = round_up(cdiv(m, CL), 8);
+  Team<CL> team;
+  team.rank = rank;
+  team.r0 = imin(m, rank * half);
+  team.r1 = imin(m, (rank + 1) * half);
+  team.red = red;
+  team.xch = xch;
+  team.xch_peer = xch;
+  team.parity = 0;
+  const double* Zpeer = Zs;
+  int peer_r0 = 0;
+  if constexpr (CL == 2) {
+    team.xch_peer = cg::this_cluster().map_shared_rank(xch, rank ^ 1);
+    Zpeer = cg::this_cluster().map_shared_rank(Zs, rank ^ 1);
+    peer_r0 = imin(m, (rank ^ 1) * half);
+  }
+  Dual<MB, CL> eng{m, smem, slot, team.r0, team.r1 - team.r0};
+  // Z(j, i) for any row j: this CTA's rows from local shared memory, the others from the peer's
+  auto zval = [&](int j, int i) -> double {
+    if (CL == 1 || (j >= team.r0 && j < team.r1)) return Zs[(j - team.r0) * zld + i];
+    return Zpeer[(j - peer_r0) * zld + i];
+  };
 
   double* ws = a.work + (size_t)inst * kDualMats * mm;
   const double* Ci = a.Ci + (size_t)inst * mm;
@@ -99,6 +189,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   double* T1 = ws + (size_t)M_T1 * mm;
   double* T2 = ws + (size_t)M_T2 * mm;
   double* T3 = ws + (size_t)M_T3 * mm;
+  double* Kg = ws + (size_t)M_X0 * mm;        // K = I + trial trial, staged through L2 for CL = 2
 
   auto store_to = [&](double* dst) {
     return [dst, m](int, int i, int j, double v) { dst[i * m + j] = v; };
@@ -109,27 +200,29 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   if (status == SSN_INSTANCE_CONVERGED) {
     // ---- eigenbasis set-up: Ce = skew(V^T (Ci/s) V), Je = skew(V^T J(V)) / s  (:106-111, :53-56)
     const int h = m / 2;
-    SSN_FOR_IJ(m, {
+    SSN_FOR_IJ(team, m, {
       T1[e] = Ci[e] / s;
       T3[e] = i < h ? V[(i + h) * m + j] : -V[(i - h) * m + j];
     })
-    __syncthreads();
+    team.sync();
     {
       MatOp A[1] = {op_t(V, m)};
       MatOp B[2] = {op_n(T1, m), op_n(T3, m)};
       auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T2 : Dl)[i * m + j] = v; };
       eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
     }
+    team.sync();
     {
       MatOp A[1] = {op_n(T2, m)};
       MatOp B[1] = {op_n(V, m)};
       auto epi = store_to(T1);
       eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
     }
+    team.sync();
     // Skew parts are exactly antisymmetric ((x - y)/2 vs (y - x)/2), which every
     // later pass relies on: precondition(r) = r / den and skew(w + t d) = w + t d
     // hold bit for bit for exactly skew r, w, d.
-    SSN_FOR_IJ(m, {
+    SSN_FOR_IJ(team, m, {
       const int et = j * m + i;
       Ce[e] = (T1[e] - T1[et]) / 2;
       Je[e] = ((Dl[e] - Dl[et]) / 2) / s;
@@ -138,7 +231,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       Qm[e] = 0.0;
       Sr[e] = (i == j) ? lam[i] : 0.0;
     })
-    __syncthreads();
+    team.sync();
 
     const double sqrt_m = sqrt(static_cast<double>(m));
     const double* SiCur = Ce;  // Si = Ci in the eigenbasis at step 0 (:121-122)
@@ -153,6 +246,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           auto epi = [&](int, int i, int j, double v) { Qm[i * m + j] = -v; };
           eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
         }
+        team.sync();
         // sandwich (:67-71): Yr = P diag(l) - Q Ce, Yi = P Ce + Q diag(l)
         {
           MatOp A[2] = {op_n(Qm, m), op_n(Pm, m)};
@@ -164,19 +258,22 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           };
           eng.template mul<2, 1, 2, C_SHARED_B>(A, B, epi);
         }
-        // Sr' = Yr P^T + Yi Q^T, Si' = Yi P^T - Yr Q^T (recover_block on m x m)
+        // Sr' = Yr P^T + Yi Q^T, Si' = Yi P^T - Yr Q^T (recover_block on m x m).  Its A
+        // operands are this CTA's own rows of Yr, Yi; its B operands P, Q are complete.
+        __syncthreads();
         {
           MatOp A[2] = {op_n(T1, m), op_n(T2, m)};
           MatOp B[2] = {op_t(Pm, m), op_t(Qm, m)};
           auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T3 : Dl)[i * m + j] = v; };
           eng.template mul<2, 2, 2, C_CPLX>(A, B, epi);
         }
+        team.sync();
         SiCur = Si;
       }
       // Sr = sym, Si = skew, gradient = Je - Si and its norm (:126-128)
       double gn2 = 0.0;
       if (step > 0) {
-        SSN_FOR_IJ(m, {
+        SSN_FOR_IJ(team, m, {
           const int et = j * m + i;
           Sr[e] = (T3[e] + T3[et]) / 2;
           const double x = (Dl[e] - Dl[et]) / 2;
@@ -186,13 +283,13 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           gn2 += gij * gij;
         })
       } else {
-        SSN_FOR_IJ(m, {
+        SSN_FOR_IJ(team, m, {
           const double gij = Je[e] - Ce[e];
           G[e] = gij;
           gn2 += gij * gij;
         })
       }
-      const double gnorm = sqrt(block_sum(gn2, red));
+      const double gnorm = sqrt(team.sum(gn2));
       const double residual = gnorm * s / sqrt_m;
       if (!(residual >= a.feas_tol / 2)) {
         if (!isfinite(residual)) status = SSN_INSTANCE_NONFINITE;
@@ -206,16 +303,16 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       if (step == 0) {
         // one preconditioner application solves H(E) = E L + L E exactly (:138-140)
         double sl = 0.0;
-        SSN_FOR_IJ(m, {
+        SSN_FOR_IJ(team, m, {
           const double z = __ddiv_rn(-G[e], lam[i] + lam[j]);
           Dd[e] = z;
           sl += G[e] * z;
         })
-        slope = block_sum(sl, red);
+        slope = team.sum(sl);
       } else {
         // PCG (:142-161)
         double rz = 0.0;
-        SSN_FOR_IJ(m, {
+        SSN_FOR_IJ(team, m, {
           const double r = -G[e];
           const double z = __ddiv_rn(r, lam[i] + lam[j]);
           Rr[e] = r;
@@ -223,60 +320,63 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           Pp[e] = z;
           rz += r * z;
         })
-        rz = block_sum(rz, red);
+        rz = team.sum(rz);
         const double tol = fmin(fmax(sqrt(residual), 1e-8), 0.1) * gnorm;
         for (int it = 0; it < a.max_cg; ++it) {
-          // H(p) = Z - Z^T with Z = P (p Sr) - Q (p Si) (:74-76); Z stays in shared memory
+          // H(p) = Z - Z^T with Z = P (p Sr) - Q (p Si) (:74-76); Z rows stay in shared memory
           {
             MatOp A[1] = {op_n(Pp, m)};
             MatOp B[2] = {op_n(Sr, m), op_n(Si, m)};
             auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T2)[i * m + j] = v; };
             eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
           }
+          team.sync();
           {
             MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
             MatOp B[2] = {op_n(T1, m), op_n(T2, m)};
-            auto epi = [&](int, int i, int j, double v) { Zs[i * zld + j] = v; };
+            const int zr0 = team.r0;
+            auto epi = [&](int, int i, int j, double v) { Zs[(i - zr0) * zld + j] = v; };
             eng.template mul<2, 2, 1, C_DIFF>(A, B, epi);
           }
+          team.sync();
           ++n_hvp;
           double curv = 0.0;
-          SSN_FOR_IJ(m, { curv += Pp[e] * (Zs[i * zld + j] - Zs[j * zld + i]); })
-          curv = block_sum(curv, red);
+          SSN_FOR_IJ(team, m, { curv += Pp[e] * (zval(i, j) - zval(j, i)); })
+          curv = team.sum(curv);
           if (!(curv > 0.0)) break;  // cg_active &= curvature > 0 (:152)
           const double alpha = rz / curv;
           double rn2 = 0.0, rz_next = 0.0;
-          SSN_FOR_IJ(m, {
-            const double hp = Zs[i * zld + j] - Zs[j * zld + i];
+          SSN_FOR_IJ(team, m, {
+            const double hp = zval(i, j) - zval(j, i);
             Dd[e] = __dadd_rn(Dd[e], __dmul_rn(alpha, Pp[e]));
             const double r = __dsub_rn(Rr[e], __dmul_rn(alpha, hp));
             Rr[e] = r;
             rn2 += r * r;
             rz_next += r * __ddiv_rn(r, lam[i] + lam[j]);
           })
-          block_sum2(rn2, rz_next, red);
+          team.sum2(rn2, rz_next);
           const double rnorm = sqrt(rn2);
           if (!(rnorm > tol)) break;  // (:155-157)
           const double beta = rz_next / rz;
-          SSN_FOR_IJ(m, {
+          SSN_FOR_IJ(team, m, {
             Pp[e] = __dadd_rn(__ddiv_rn(Rr[e], lam[i] + lam[j]), __dmul_rn(beta, Pp[e]));
           })
-          __syncthreads();
+          team.sync();
           rz = rz_next;
         }
         double sl = 0.0;
-        SSN_FOR_IJ(m, { sl += G[e] * Dd[e]; })
-        slope = block_sum(sl, red);
+        SSN_FOR_IJ(team, m, { sl += G[e] * Dd[e]; })
+        slope = team.sum(sl);
         // non-descent fallback to the preconditioned gradient (:163-164)
         if (slope >= 0.0) {
           ++n_fallback;
           double s2 = 0.0;
-          SSN_FOR_IJ(m, {
+          SSN_FOR_IJ(team, m, {
             const double z = __ddiv_rn(-G[e], lam[i] + lam[j]);
             Dd[e] = z;
             s2 += G[e] * z;
           })
-          slope = block_sum(s2, red);
+          slope = team.sum(s2);
         }
       }
 
@@ -286,23 +386,32 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       for (int bt = 0; bt < a.max_backtrack; ++bt) {
         ++n_trial;
         double first = 0.0;
-        SSN_FOR_IJ(m, {
+        SSN_FOR_IJ(team, m, {
           const double dl = __dmul_rn(t, Dd[e]);
           Dl[e] = dl;
           first += G[e] * dl;
           Wt[e] = __dadd_rn(Wm[e], dl);      // == skew(omega + delta) for exactly skew omega, delta
         })
-        first = block_sum(first, red);
+        first = team.sum(first);
         // K = I + trial trial, positive-definiteness test + inverse in shared memory
         double* Ks = smem;
         const int mp16 = round_up(m, 16), kld = frag_ld(mp16);
-        {
+        if constexpr (CL == 1) {
           MatOp A[1] = {op_n(Wt, m)};
           MatOp B[1] = {op_n(Wt, m)};
           auto epi = [&](int, int i, int j, double v) {
             Ks[i * kld + j] = __dadd_rn(i == j ? 1.0 : 0.0, v);
           };
           eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+        } else {
+          // each CTA forms its rows of K in L2; both then invert the full K
+          MatOp A[1] = {op_n(Wt, m)};
+          MatOp B[1] = {op_n(Wt, m)};
+          auto epi = [&](int, int i, int j, double v) { Kg[i * m + j] = __dadd_rn(i == j ? 1.0 : 0.0, v); };
+          eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+          team.sync();
+          for (int i = (int)(threadIdx.x >> 5); i < m; i += kWarps)
+            for (int j = (int)(threadIdx.x & 31); j < m; j += 32) Ks[i * kld + j] = Kg[i * m + j];
         }
         for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {   // identity padding up to mp16
           const int i = e / mp16, j = e - i * mp16;
@@ -311,9 +420,9 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
         __syncthreads();
         const bool valid = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
         if (valid) {
-          SSN_FOR_IJ(m, { Pt[e] = Ks[i * kld + j]; })
+          SSN_FOR_IJ(team, m, { Pt[e] = Ks[i * kld + j]; })
         }
-        __syncthreads();
+        team.sync();
         if (valid) {
           // V = P_trial delta; dSr = delta Sr, dSi = delta Si (:177-178)
           {
@@ -322,12 +431,14 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
             auto epi = store_to(T1);
             eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
           }
+          __syncthreads();
           {
             MatOp A[1] = {op_n(Dl, m)};
             MatOp B[2] = {op_n(Sr, m), op_n(SiCur, m)};
             auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T2 : T3)[i * m + j] = v; };
             eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
           }
+          team.sync();
           // tail = <V, dSr + trial dSi> (line_change, hvp_fused.cu:259-371)
           double tail = 0.0;
           {
@@ -339,7 +450,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
             };
             eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
           }
-          tail = block_sum(tail, red);
+          tail = team.sum(tail);
           const double change = __dadd_rn(first, tail);
           if (change <= 1e-4 * t * slope) {
             double* tmp = Wm;
@@ -362,33 +473,38 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
     double* Wout = a.omega + (size_t)inst * mm;
     double* Pout = a.P + (size_t)inst * mm;
     double* Qout = a.Q + (size_t)inst * mm;
+    team.sync();
     {
       MatOp A[1] = {op_n(V, m)};
-      MatOp B[1] = {op_n(Wm, m)};
-      auto epi = store_to(T1);
-      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
-    }
-    {
-      MatOp A[1] = {op_n(T1, m)};
-      MatOp B[1] = {op_t(V, m)};
-      auto epi = store_to(T2);
-      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
-    }
-    SSN_FOR_IJ(m, { Wout[e] = (T2[e] - T2[j * m + i]) / 2; })
-    {
-      MatOp A[1] = {op_n(V, m)};
-      MatOp B[2] = {op_n(Pm, m), op_n(Qm, m)};
+      MatOp B[2] = {op_n(Wm, m), op_n(Pm, m)};
       auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T3)[i * m + j] = v; };
       eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
     }
+    __syncthreads();
+    {
+      MatOp A[1] = {op_n(V, m)};
+      MatOp B[1] = {op_n(Qm, m)};
+      auto epi = store_to(T2);
+      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+    }
+    __syncthreads();
     {
       MatOp A[2] = {op_n(T1, m), op_n(T3, m)};
       MatOp B[1] = {op_t(V, m)};
-      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Pout : Qout)[i * m + j] = v; };
+      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Dl : Pout)[i * m + j] = v; };
       eng.template mul<2, 1, 2, C_SHARED_B>(A, B, epi);
     }
+    __syncthreads();
+    {
+      MatOp A[1] = {op_n(T2, m)};
+      MatOp B[1] = {op_t(V, m)};
+      auto epi = store_to(Qout);
+      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+    }
+    team.sync();
+    SSN_FOR_IJ(team, m, { Wout[e] = (Dl[e] - Dl[j * m + i]) / 2; })
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && rank == 0) {
     a.iterations[inst] = iterations;
     a.status[inst] = status;
     if (a.counters) {
@@ -398,29 +514,58 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       a.counters[inst * 4 + 3] = n_fallback;
     }
   }
+  if constexpr (CL == 2) cg::this_cluster().sync();   // no CTA leaves while its peer may read its shared memory
 }
 
 static size_t dual_smem_bytes(int MB) {
   const int region = imax(8 * slot_doubles(MB), spd_region_doubles(32 * MB));
-  return sizeof(double) * ((size_t)region + 2 * kWarps + kMaxM) + 16;
+  return sizeof(double) * ((size_t)region + 2 * kWarps + kMaxM + 8) + 16;
 }
 
-template <int MB>
+static int sm_count() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+template <int MB, int CL>
 static cudaError_t launch_dual_mb(const DualArgs& args, int batch, cudaStream_t stream) {
   const size_t smem = dual_smem_bytes(MB);
-  cudaError_t err = cudaFuncSetAttribute(dual_kernel<MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t err = cudaFuncSetAttribute(dual_kernel<MB, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;
-  dual_kernel<MB><<<batch, kThreads, smem, stream>>>(args);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(batch * CL);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  err = cudaLaunchKernelEx(&cfg, dual_kernel<MB, CL>, args);
+  if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
 
+// Two CTAs per instance when the batch leaves half the SMs idle and m is large
+// enough for the row split to pay; one otherwise.
+int dual_cluster_size(int batch, int m) { return (m >= 48 && 2 * batch <= sm_count()) ? 2 : 1; }
+
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
+  const bool two = dual_cluster_size(batch, args.m) == 2;
   switch (bucket_of(args.m)) {
-    case 1: return launch_dual_mb<1>(args, batch, stream);
-    case 2: return launch_dual_mb<2>(args, batch, stream);
-    case 3: return launch_dual_mb<3>(args, batch, stream);
-    default: return launch_dual_mb<4>(args, batch, stream);
+    case 1: return launch_dual_mb<1, 1>(args, batch, stream);
+    case 2: return two ? launch_dual_mb<2, 2>(args, batch, stream) : launch_dual_mb<2, 1>(args, batch, stream);
+    case 3: return two ? launch_dual_mb<3, 2>(args, batch, stream) : launch_dual_mb<3, 1>(args, batch, stream);
+    default: return two ? launch_dual_mb<4, 2>(args, batch, stream) : launch_dual_mb<4, 1>(args, batch, stream);
   }
 }
 
