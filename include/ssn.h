@@ -173,6 +173,18 @@ int ssn_newton(const double* Ci, const double* values, const double* vectors, co
  */
 int ssn_probe_fp64_mma(double* sink, int iters, double* flops, ssn_stream_t stream);
 
+/*
+ * Check of the INT8 tensor-core path with no counterpart in the reference:
+ * one CTA computes C[128 x n] = A[128 x k] * B[n x k]^T (row-major int8 in,
+ * int32 out) with tcgen05.mma kind::i8 from no-swizzle K-major shared-memory
+ * operands into a TMEM accumulator.  The split-precision Gram and recovery
+ * kernels are built from the same descriptors.  16 <= n <= 256, n % 16 == 0,
+ * 32 <= k <= 256, k % 32 == 0, A and B 16-byte aligned.  *stall (device) is
+ * set to 1 if the MMA completion was not observed within the wait bound.
+ */
+int ssn_probe_s8_mma(const int8_t* A, const int8_t* B, int32_t* C, int n, int k, int* stall,
+                     ssn_stream_t stream);
+
 /* ---- component operations (mirrors of the reference kernel wrappers) ----
  * All matrices [batch, m, m] contiguous FP64; vectors [batch] or [batch, m]. */
 

@@ -299,6 +299,13 @@ int ssn_probe_fp64_mma(double* sink, int iters, double* flops, ssn_stream_t stre
   return cuda_status(launch_probe_fp64_mma(sink, iters, flops, reinterpret_cast<cudaStream_t>(stream)));
 }
 
+int ssn_probe_s8_mma(const int8_t* A, const int8_t* B, int32_t* C, int n, int k, int* stall,
+                     ssn_stream_t stream) {
+  if (!A || !B || !C || !stall || !aligned16(A) || !aligned16(B)) return SSN_ERR_INVALID_ARGUMENT;
+  if (n < 16 || n > 256 || n % 16 != 0 || k < 32 || k > 256 || k % 32 != 0) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_probe_s8_mma(A, B, C, n, k, stall, reinterpret_cast<cudaStream_t>(stream)));
+}
+
 #define SSN_CHECK_MATS(...)                                                   \
   do {                                                                        \
     const void* ps_[] = {__VA_ARGS__};                                        \

@@ -38,6 +38,8 @@ cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, doubl
                         cudaStream_t stream);
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
 cudaError_t launch_probe_fp64_mma(double* sink, int iters, double* flops, cudaStream_t stream);
+cudaError_t launch_probe_s8_mma(const int8_t* A, const int8_t* B, int32_t* C, int n, int k, int* stall,
+                                cudaStream_t stream);
 
 size_t gram_partial_doubles(int batch, int rows, int m);
 // number of row splits launch_gram uses for this shape when capped at max_splits

@@ -38,6 +38,7 @@ PROTOTYPES = {
     "ssn_newton_workspace_bytes": (_SZ, [_I, _I]),
     "ssn_newton": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
     "ssn_probe_fp64_mma": (_I, [_P, _I, _P, _P]),
+    "ssn_probe_s8_mma": (_I, [_P, _P, _P, _I, _I, _P, _P]),
     "ssn_inner_products": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
     "ssn_outer_skew": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
     "ssn_sandwich_front": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _P]),
