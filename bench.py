@@ -30,6 +30,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "symplectic-stiefel-nearness_b200"))
 
 METRIC = "solves/s, 64×(8192×96) batch, all pass r_F/r_G/δ checks: split-prec vs FP64"
+PRECISION_NOTE = {
+    "split": "split-precision form: FP32 Jacobi eigenbasis (re-orthogonalised in FP64) + FP64 Newton-CG, "
+             "FP64 in and out",
+    "fp64": "fp64 (plain FP64 form)",
+}
 N_DEFAULT, K_DEFAULT, BATCH_DEFAULT = 4096, 48, 64
 
 
@@ -45,6 +50,9 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--precision", choices=["split", "fp64", "both"], default="both",
+                   help="form timed for `value` (split when both; the FP64 form is then reported beside it)")
+    p.add_argument("--eig-sweeps", type=int, default=0, help="split form: Jacobi sweeps (0 = library default)")
     return p.parse_args()
 
 
@@ -203,23 +211,22 @@ def run_ours(args):
     newton_bytes = lib.ssn_newton_workspace_bytes(B, m)
     eigh_bytes = lib.ssn_eigh_workspace_bytes(B, m)
     ws = torch.empty(max(gram_bytes, newton_bytes, eigh_bytes), dtype=torch.uint8, device=dev)
-    opt = N.options()
     stride = 2 * n * m
     A_ptr, D_ptr = T.data_ptr(), T.data_ptr() + 8 * n * m
     X_top, X_bot = X.data_ptr(), X.data_ptr() + 8 * n * m
 
-    def phases(ev=None):
+    def phases(opt, ev=None):
         if ev: ev[0].record(stream)
         N.check(lib.ssn_gram(A_ptr, D_ptr, stride, Cr.data_ptr(), Ci.data_ptr(), B, n, m,
                              ws.data_ptr(), gram_bytes, sh), "gram")
         if ev: ev[1].record(stream)
         N.check(lib.ssn_eigh(Cr.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(),
-                             sweeps.data_ptr(), B, m, ws.data_ptr(), eigh_bytes, sh), "eigh")
+                             sweeps.data_ptr(), B, m, ws.data_ptr(), eigh_bytes, N.ctypes.byref(opt), sh), "eigh")
         if ev: ev[2].record(stream)
-        N.check(lib.ssn_newton(Ci.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(), None,
-                               omega.data_ptr(), Pf.data_ptr(), Qf.data_ptr(), iters.data_ptr(),
-                               status.data_ptr(), counters.data_ptr(), B, m, ws.data_ptr(), newton_bytes,
-                               N.ctypes.byref(opt), sh), "newton")
+        N.check(lib.ssn_newton(Cr.data_ptr(), Ci.data_ptr(), values.data_ptr(), vectors.data_ptr(),
+                               scale.data_ptr(), None, omega.data_ptr(), Pf.data_ptr(), Qf.data_ptr(),
+                               iters.data_ptr(), status.data_ptr(), counters.data_ptr(), B, m, ws.data_ptr(),
+                               newton_bytes, N.ctypes.byref(opt), sh), "newton")
         if ev: ev[3].record(stream)
         N.check(lib.ssn_recover(A_ptr, D_ptr, stride, Pf.data_ptr(), Qf.data_ptr(), X_top, X_bot, stride,
                                 B, n, m, sh), "recover")
@@ -237,51 +244,73 @@ def run_ours(args):
         e1.synchronize()
         peak = max(peak, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
 
-    for _ in range(max(3, args.warmup)):
-        phases()
-    torch.cuda.synchronize(dev)
+    def timed_form(precision):
+        """K timed steps of one precision form; returns its measurements (all ranks)."""
+        opt = N.options(precision=precision, eig_sweeps=args.eig_sweeps)
+        for _ in range(max(3, args.warmup)):
+            phases(opt)
+        torch.cuda.synchronize(dev)
+        K = args.steps
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
+        sampler = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+        sampler.start()
+        time.sleep(0.3)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for s in range(K):
+            phases(opt, evs[s])
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        clocks = sampler.stop()
+        total_ms = start.elapsed_time(end)
+        phase_ms = [0.0] * 4
+        for ev in evs:
+            for i in range(4):
+                phase_ms[i] += ev[i].elapsed_time(ev[i + 1])
+        if world > 1:
+            t = torch.tensor([total_ms] + phase_ms, dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms, phase_ms = float(t[0]), [float(x) for x in t[1:]]
 
-    K = args.steps
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
-    sampler = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
-    sampler.start()
-    time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for s in range(K):
-        phases(evs[s])
-    end.record(stream)
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    clocks = sampler.stop()
-    total_ms = start.elapsed_time(end)
-    phase_ms = [0.0] * 4
-    for ev in evs:
-        for i in range(4):
-            phase_ms[i] += ev[i].elapsed_time(ev[i + 1])
-    if world > 1:
-        t = torch.tensor([total_ms] + phase_ms, dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, phase_ms = float(t[0]), [float(x) for x in t[1:]]
+        # correctness of the timed outputs: every instance converged and passes the checks
+        st = status.cpu()
+        cert = certify(T, X)
+        passed = bool(cert["passed"].all()) and bool((st == 0).all())
+        worst = {key: float(cert[key].max()) for key in ("feasibility", "stationarity", "delta")}
+        cnt = counters.cpu().to(torch.int64)
 
-    # correctness of the timed outputs: every instance converged and passes the checks
-    st = status.cpu()
-    cert = certify(T, X)
-    passed = bool(cert["passed"].all()) and bool((st == 0).all())
-    worst = {key: float(cert[key].max()) for key in ("feasibility", "stationarity", "delta")}
-    cnt = counters.cpu().to(torch.int64)
+        # algorithmic work per launch
+        n_steps, n_hvp, n_trial = (int(cnt[:, i].sum()) for i in range(3))
+        mm3 = 2.0 * m ** 3
+        extra = (4 * max(0, n_steps - B) + 9 * B) if precision == "split" else 0   # full-Gram sandwich, set-up
+        newton_flops = (4 * n_hvp + 7 * max(0, n_steps - B) + 6 * n_trial + 9 * B + extra) * mm3
+        tall_flops = 8.0 * n * m * m * B             # per Gram or per recovery launch
+        per_launch = {"gram": (tall_flops, phase_ms[0] / K), "eigh": (None, phase_ms[1] / K),
+                      "newton": (newton_flops, phase_ms[2] / K), "recover": (tall_flops, phase_ms[3] / K)}
+        phases_out = {}
+        for name, (f, t_ms) in per_launch.items():
+            phases_out[name] = {"ms": t_ms, "tflops": (f / (t_ms * 1e-3) / 1e12) if f else None,
+                                "frac_of_fp64_peak": (f / (t_ms * 1e-3) / 1e12 / peak) if f else None}
+        phases_out["newton"]["work"] = {"newton_steps": n_steps, "hvps": n_hvp, "trials": n_trial,
+                                        "algorithmic_flops": newton_flops}
+        sw = sweeps.cpu()
+        phases_out["eigh"]["jacobi_sweeps"] = {"max": int(sw.max()), "mean": float(sw.double().mean())}
+        phases_out["hbm_floor_ms"] = 48.0 * n * m * B / 6549.8e9 * 1e3
+        ms_step = total_ms / K
+        return {"precision": precision, "ms_step": ms_step, "value": world * B / (ms_step * 1e-3),
+                "passed": passed, "worst": worst, "clocks": clocks, "per_launch": per_launch,
+                "phases": phases_out, "K": K, "X": X.clone(), "omega": omega.clone(), "iters": iters.clone()}
 
-    # algorithmic work per launch
-    n_steps, n_hvp, n_trial = (int(cnt[:, i].sum()) for i in range(3))
-    mm3 = 2.0 * m ** 3
-    newton_flops = (4 * n_hvp + 7 * max(0, n_steps - B) + 6 * n_trial + 9 * B) * mm3
-    tall_flops = 8.0 * n * m * m * B             # per Gram or per recovery launch
-    per_launch = {"gram": (tall_flops, phase_ms[0] / K), "eigh": (None, phase_ms[1] / K),
-                  "newton": (newton_flops, phase_ms[2] / K), "recover": (tall_flops, phase_ms[3] / K)}
+    forms = ["split", "fp64"] if args.precision == "both" else [args.precision]
+    results = {f: timed_form(f) for f in forms}
+    head = results[forms[0]]
+    K = head["K"]
+    per_launch = head["per_launch"]
     dominant = max(per_launch, key=lambda kk: per_launch[kk][1])
     fl, ms = per_launch[dominant]
     achieved = (fl / (ms * 1e-3) / 1e12) if fl else None
@@ -289,18 +318,24 @@ def run_ours(args):
                 "frac": (achieved / peak) if achieved else None, "traffic": None, "kernel": dominant,
                 "peak_source": "FP64 DMMA rate measured in this run (ssn_probe_fp64_mma); "
                                "no FP64 figure in the driver's peak file"}
-    phases_out = {}
-    for name, (f, t_ms) in per_launch.items():
-        phases_out[name] = {"ms": t_ms, "tflops": (f / (t_ms * 1e-3) / 1e12) if f else None,
-                            "frac_of_fp64_peak": (f / (t_ms * 1e-3) / 1e12 / peak) if f else None}
-    phases_out["newton"]["work"] = {"newton_steps": n_steps, "hvps": n_hvp, "trials": n_trial,
-                                    "algorithmic_flops": newton_flops}
-    sw = sweeps.cpu()
-    phases_out["eigh"]["jacobi_sweeps"] = {"max": int(sw.max()), "mean": float(sw.double().mean())}
-    phases_out["hbm_floor_ms"] = 48.0 * n * m * B / 6549.8e9 * 1e3
+    passed, worst, clocks, phases_out = head["passed"], head["worst"], head["clocks"], head["phases"]
+    ms_step, value = head["ms_step"], head["value"]
+    compare = None
+    if len(forms) == 2:
+        fp = results["fp64"]
 
-    ms_step = total_ms / K
-    value = world * B / (ms_step * 1e-3)
+        def relerr(a, b):
+            num = torch.linalg.vector_norm((a - b).flatten(1), dim=1)
+            return float((num / torch.linalg.vector_norm(b.flatten(1), dim=1).clamp_min(1e-300)).max())
+
+        compare = {"fp64_form": {"value": fp["value"], "ms_per_step": fp["ms_step"], "all_pass": fp["passed"],
+                                 "worst": fp["worst"], "phases": fp["phases"], "clocks": fp["clocks"]},
+                   "split_over_fp64": head["value"] / fp["value"],
+                   "split_vs_fp64_max_rel": {"X": relerr(head["X"], fp["X"]),
+                                             "omega": relerr(head["omega"], fp["omega"]),
+                                             "iterations_max_abs_diff":
+                                                 int((head["iters"] - fp["iters"]).abs().max())}}
+        passed = passed and fp["passed"]
 
     # end to end through the public API: pinned host T -> device -> host X, omega, iterations
     e2e_ms = []
@@ -308,7 +343,7 @@ def run_ours(args):
     for i in range(2 + max(1, args.e2e_steps)):   # two untimed calls fill the pinned-buffer caches
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        X_host, W_host, I_host = sp.solve(T_host)
+        X_host, W_host, I_host = sp.solve(T_host, precision=forms[0])
         e1.record(stream)
         e1.synchronize()
         if i > 1:
@@ -335,12 +370,14 @@ def run_ours(args):
             "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded N(0,1/(2n)) targets (reference generator rule)",
-            "config": dict(workload(args), precision="fp64 (plain FP64 form)", parallelism=f"replicas x{world}"),
+            "config": dict(workload(args), precision=PRECISION_NOTE[forms[0]], parallelism=f"replicas x{world}"),
             "all_pass": passed, "worst": worst, "clocks": clocks,
             "e2e": {"value": world * B / (e2e_step * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step,
                     "link": link},
             "gpu_launches": 6 * K, "roofline": roofline, "phases": phases_out}
+    if compare:
+        line.update(compare)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, args.cpu_seconds)
     if rank == 0:

@@ -52,13 +52,29 @@ enum {
   SSN_INSTANCE_EIGH = 6
 };
 
+/* Arithmetic of a solve (ssn_options.precision). */
+enum {
+  /* Plain FP64 throughout: the reference's algorithm step for step (same
+   * iterates up to rounding), with a fully converged FP64 Jacobi eigenbasis. */
+  SSN_PRECISION_FP64 = 0,
+  /* Split precision: the eigenbasis of the scaled Gram comes from a few FP32
+   * Jacobi sweeps (ssn_options.eig_sweeps), is re-orthogonalised in FP64, and
+   * the Newton iteration uses the full rotated Gram, so the solution is the
+   * same dual optimum; Newton, line search and residuals stay FP64.  Inputs
+   * and outputs are FP64 and every result is held to the same acceptance
+   * bounds as the FP64 form. */
+  SSN_PRECISION_SPLIT = 1
+};
+
 /* Solver constants; defaults follow dual_recommended_hvp.py:13-16. */
 typedef struct {
   int max_newton;    /* 100 */
   int max_cg;        /* 150 */
   int max_backtrack; /* 40  */
   double feas_tol;   /* 1e-8: an instance is done when residual < feas_tol / 2 */
-  int reserved[8];
+  int precision;     /* SSN_PRECISION_FP64 (default) or SSN_PRECISION_SPLIT */
+  int eig_sweeps;    /* split form: Jacobi sweeps of the rough eigenbasis (0 = default 3, max 24) */
+  int reserved[6];
 } ssn_options;
 
 /* Library version as 10000*major + 100*minor + patch. */
@@ -74,6 +90,7 @@ size_t ssn_workspace_bytes(int batch, int n, int m);
 /*
  * Full solve: T [batch, 2n, m] -> X [batch, 2n, m], omega [batch, m, m],
  * iterations int64 [batch] (Newton updates per instance), status int32 [batch].
+ * opt->precision selects the plain FP64 form or the split-precision form.
  * Replaces symplectic_projection.solve (dual_recommended_hvp.py:231-242),
  * i.e. gram_chunks (:79-96) + dual_batch (:99-191) + recover_matmul (:194-228),
  * with device-resident input and output (no chunked PCIe staging).
@@ -128,19 +145,22 @@ int ssn_recover(const double* A, const double* D, int64_t ab_stride,
 /*
  * Symmetric eigendecomposition of the scaled Gram matrix, Cr / s = V diag(w) V^T
  * with s = max(1, trace(Cr)/m) (dual_recommended_hvp.py:106-108, where the
- * reference calls torch.linalg.eigh).  Cyclic two-sided Jacobi in FP64;
- * eigenvalues ascending.  scale and sweeps (Jacobi sweeps per instance) may be
- * NULL.  The workspace (ssn_eigh_workspace_bytes) holds the rotation log.
+ * reference calls torch.linalg.eigh).  Cyclic two-sided Jacobi; eigenvalues
+ * ascending.  opt NULL or opt->precision == SSN_PRECISION_FP64: FP64 rotations
+ * until convergence.  SSN_PRECISION_SPLIT: opt->eig_sweeps FP32 sweeps, a rough
+ * basis for ssn_newton's split form (V only approximately orthogonal).
+ * scale and sweeps (Jacobi sweeps per instance) may be NULL.  The workspace
+ * (ssn_eigh_workspace_bytes) holds the rotation log.
  */
 size_t ssn_eigh_workspace_bytes(int batch, int m);
 int ssn_eigh(const double* Cr, double* values, double* vectors, double* scale,
              int32_t* sweeps, int batch, int m, void* workspace, size_t workspace_bytes,
-             ssn_stream_t stream);
+             const ssn_options* opt, ssn_stream_t stream);
 
 /*
  * Dual Newton-CG on given Gram matrices: (Cr, Ci) -> omega, and the final
  * inverse parts P + iQ = (I + i omega)^-1, all in the original basis, plus
- * iterations and status.  Replaces dual_batch (dual_recommended_hvp.py:99-191)
+ * iterations and status (either precision form, opt->precision).  Replaces dual_batch (dual_recommended_hvp.py:99-191)
  * with the `final` cache (:131-134).  Needs ssn_dual_workspace_bytes.
  */
 size_t ssn_dual_workspace_bytes(int batch, int m);
@@ -154,12 +174,14 @@ int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, doubl
  * ssn_eigh (values, vectors, scale, and its per-instance status eig_status,
  * which may be NULL).  counters (may be NULL) receives int32 [batch, 4]:
  * Newton steps run, Hessian-vector products, line-search trials, fallbacks.
+ * Cr (the unscaled Gram) is read only by the split form (opt->precision ==
+ * SSN_PRECISION_SPLIT, where it is required) and may be NULL otherwise.
  * Replaces dual_batch (dual_recommended_hvp.py:109-191) after the eigh call.
  * Needs ssn_newton_workspace_bytes.
  */
 size_t ssn_newton_workspace_bytes(int batch, int m);
-int ssn_newton(const double* Ci, const double* values, const double* vectors, const double* scale,
-               const int32_t* eig_status, double* omega, double* P, double* Q,
+int ssn_newton(const double* Cr, const double* Ci, const double* values, const double* vectors,
+               const double* scale, const int32_t* eig_status, double* omega, double* P, double* Q,
                int64_t* iterations, int32_t* status, int32_t* counters, int batch, int m,
                void* workspace, size_t workspace_bytes, const ssn_options* opt,
                ssn_stream_t stream);

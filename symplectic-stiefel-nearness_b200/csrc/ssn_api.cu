@@ -76,6 +76,8 @@ DualLayout dual_layout(int batch, int m) {
   return L;
 }
 
+constexpr int kDefaultEigSweeps = 3;
+
 void fill_options(const ssn_options* opt, DualArgs& a) {
   ssn_options d;
   ssn_default_options(&d);
@@ -84,13 +86,29 @@ void fill_options(const ssn_options* opt, DualArgs& a) {
   a.max_cg = opt->max_cg;
   a.max_backtrack = opt->max_backtrack;
   a.feas_tol = opt->feas_tol;
+  a.approx_basis = opt->precision == SSN_PRECISION_SPLIT ? 1 : 0;
+  a.orthogonalize = a.approx_basis;
 }
+
+bool split_form(const ssn_options* opt) { return opt && opt->precision == SSN_PRECISION_SPLIT; }
+int eig_sweeps(const ssn_options* opt) { return opt && opt->eig_sweeps > 0 ? opt->eig_sweeps : kDefaultEigSweeps; }
 
 bool options_ok(const ssn_options* opt) {
   if (!opt) return true;
   return opt->max_newton >= 1 && opt->max_newton <= 100000 && opt->max_cg >= 1 &&
          opt->max_cg <= 100000 && opt->max_backtrack >= 1 && opt->max_backtrack <= 1074 &&
-         opt->feas_tol > 0.0;
+         opt->feas_tol > 0.0 &&
+         (opt->precision == SSN_PRECISION_FP64 || opt->precision == SSN_PRECISION_SPLIT) &&
+         opt->eig_sweeps >= 0 && opt->eig_sweeps <= 24;
+}
+
+// Eigenbasis of the scaled Gram for either precision form.
+cudaError_t eigenbasis(const ssn_options* opt, const double* Cr, double* values, double* vectors, double* scale,
+                       int32_t* sweeps, int32_t* status, int batch, int m, void* ws, cudaStream_t stream) {
+  if (split_form(opt))
+    return launch_eigh_approx(Cr, values, vectors, scale, sweeps, status, batch, m, ws, eig_sweeps(opt), true,
+                              stream);
+  return launch_eigh(Cr, values, vectors, scale, sweeps, status, batch, m, ws, stream);
 }
 
 }  // namespace
@@ -154,7 +172,7 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
   const double* D = T + (size_t)n * m;
   cudaError_t e = launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
-  e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m, ws + L.eig_ws, stream);
+  e = eigenbasis(opt, Cr, values, vectors, scale, nullptr, eig_status, batch, m, ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   DualArgs a{};
   a.m = m;
@@ -212,12 +230,13 @@ size_t ssn_eigh_workspace_bytes(int batch, int m) {
 }
 
 int ssn_eigh(const double* Cr, double* values, double* vectors, double* scale, int32_t* sweeps,
-             int batch, int m, void* workspace, size_t workspace_bytes, ssn_stream_t stream) {
-  if (!shape_ok(batch, m) || !Cr || !values || !vectors) return SSN_ERR_INVALID_ARGUMENT;
+             int batch, int m, void* workspace, size_t workspace_bytes, const ssn_options* opt,
+             ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !Cr || !values || !vectors || !options_ok(opt)) return SSN_ERR_INVALID_ARGUMENT;
   if (!workspace || workspace_bytes < eigh_workspace_bytes(batch, m) || !aligned16(workspace))
     return SSN_ERR_WORKSPACE;
-  return cuda_status(launch_eigh(Cr, values, vectors, scale, sweeps, nullptr, batch, m, workspace,
-                                 reinterpret_cast<cudaStream_t>(stream)));
+  return cuda_status(eigenbasis(opt, Cr, values, vectors, scale, sweeps, nullptr, batch, m, workspace,
+                                reinterpret_cast<cudaStream_t>(stream)));
 }
 
 size_t ssn_dual_workspace_bytes(int batch, int m) {
@@ -239,8 +258,8 @@ int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, doubl
   double* vectors = reinterpret_cast<double*>(ws + L.vectors);
   double* scale = reinterpret_cast<double*>(ws + L.scale);
   int32_t* eig_status = reinterpret_cast<int32_t*>(ws + L.eig_status);
-  cudaError_t e = launch_eigh(Cr, values, vectors, scale, nullptr, eig_status, batch, m,
-                              ws + L.eig_ws, stream);
+  cudaError_t e = eigenbasis(opt, Cr, values, vectors, scale, nullptr, eig_status, batch, m,
+                             ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   DualArgs a{};
   a.m = m;
@@ -266,19 +285,20 @@ size_t ssn_newton_workspace_bytes(int batch, int m) {
   return sizeof(double) * (size_t)batch * kDualMats * m * m;
 }
 
-int ssn_newton(const double* Ci, const double* values, const double* vectors, const double* scale,
-               const int32_t* eig_status, double* omega, double* P, double* Q, int64_t* iterations,
-               int32_t* status, int32_t* counters, int batch, int m, void* workspace,
+int ssn_newton(const double* Cr, const double* Ci, const double* values, const double* vectors,
+               const double* scale, const int32_t* eig_status, double* omega, double* P, double* Q,
+               int64_t* iterations, int32_t* status, int32_t* counters, int batch, int m, void* workspace,
                size_t workspace_bytes, const ssn_options* opt, ssn_stream_t stream) {
   if (!shape_ok(batch, m) || !Ci || !values || !vectors || !scale || !omega || !P || !Q ||
       !iterations || !status || !options_ok(opt) || !aligned16(Ci) || !aligned16(vectors))
     return SSN_ERR_INVALID_ARGUMENT;
+  if (split_form(opt) && (!Cr || !aligned16(Cr))) return SSN_ERR_INVALID_ARGUMENT;
   if (!workspace || workspace_bytes < ssn_newton_workspace_bytes(batch, m) || !aligned16(workspace))
     return SSN_ERR_WORKSPACE;
   DualArgs a{};
   a.m = m;
   fill_options(opt, a);
-  a.Cr = nullptr;
+  a.Cr = Cr;
   a.Ci = Ci;
   a.values = values;
   a.vectors = vectors;

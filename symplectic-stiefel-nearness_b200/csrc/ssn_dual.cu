@@ -40,6 +40,9 @@ constexpr uint32_t C_SHARED_A = coef_bit(0, 0, 0, 1) | coef_bit(1, 0, 1, 1);
 constexpr uint32_t C_DIFF = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 2);
 constexpr uint32_t C_CPLX = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1) | coef_bit(1, 1, 0, 1) |
                             coef_bit(1, 0, 1, 2);
+// (P + iQ)(C + iE): out0 = P C - Q E, out1 = P E + Q C
+constexpr uint32_t C_SANDF = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 2) | coef_bit(1, 0, 1, 1) |
+                             coef_bit(1, 1, 0, 1);
 
 // Warp-tile shape of a CL-way row split for bucket MB: each CTA computes at most
 // round_up(32*MB / CL, 8) rows of every m x m product.
@@ -200,28 +203,94 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   if (status == SSN_INSTANCE_CONVERGED) {
     // ---- eigenbasis set-up: Ce = skew(V^T (Ci/s) V), Je = skew(V^T J(V)) / s  (:106-111, :53-56)
     const int h = m / 2;
+    double* CrE = ws + (size_t)M_X2 * mm;       // approximate basis: sym(V^T (Cr/s) V)
+    if (a.approx_basis && a.orthogonalize) {
+      // V <- V (3I - V^T V) / 2 twice: vectors from FP32 rotations become orthogonal to FP64 rounding
+      double* Vb[2] = {ws + (size_t)M_X2 * mm, ws + (size_t)M_X1 * mm};
+      const double* Vin = V;
+      for (int it = 0; it < 2; ++it) {
+        {
+          MatOp A[1] = {op_t(Vin, m)};
+          MatOp B[1] = {op_n(Vin, m)};
+          auto epi = store_to(T1);
+          eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+        }
+        team.sync();
+        double* Vout = Vb[it];
+        {
+          MatOp A[1] = {op_n(Vin, m)};
+          MatOp B[1] = {op_n(T1, m)};
+          auto epi = [&](int, int i, int j, double v) {
+            const int e = i * m + j;
+            Vout[e] = 1.5 * Vin[e] - 0.5 * v;
+          };
+          eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+        }
+        team.sync();
+        Vin = Vout;
+      }
+      V = Vin;                                  // == M_X1
+    }
     SSN_FOR_IJ(team, m, {
       T1[e] = Ci[e] / s;
       T3[e] = i < h ? V[(i + h) * m + j] : -V[(i - h) * m + j];
     })
     team.sync();
-    {
-      MatOp A[1] = {op_t(V, m)};
-      MatOp B[2] = {op_n(T1, m), op_n(T3, m)};
-      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T2 : Dl)[i * m + j] = v; };
-      eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
+    if (a.approx_basis) {
+      double* Kt = ws + (size_t)M_X0 * mm;
+      const double* Crb = a.Cr + (size_t)inst * mm;
+      {
+        MatOp A[1] = {op_t(V, m)};
+        MatOp B[2] = {op_n(T1, m), op_n(Crb, m)};
+        auto epi = [&](int o, int i, int j, double v) {
+          if (o == 0) T2[i * m + j] = v;
+          else Kt[i * m + j] = v / s;
+        };
+        eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
+      }
+      __syncthreads();
+      {
+        MatOp A[1] = {op_t(V, m)};
+        MatOp B[1] = {op_n(T3, m)};
+        auto epi = store_to(Dl);
+        eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+      }
+      team.sync();
+      {
+        MatOp A[2] = {op_n(T2, m), op_n(Kt, m)};
+        MatOp B[1] = {op_n(V, m)};
+        auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T3)[i * m + j] = v; };
+        eng.template mul<2, 1, 2, C_SHARED_B>(A, B, epi);
+      }
+      team.sync();
+      SSN_FOR_IJ(team, m, {
+        const int et = j * m + i;
+        const double c = (T3[e] + T3[et]) / 2;
+        CrE[e] = c;
+        Sr[e] = c;
+      })
+      team.sync();
+      for (int i = threadIdx.x; i < m; i += kThreads) lam[i] = CrE[i * m + i];
+    } else {
+      {
+        MatOp A[1] = {op_t(V, m)};
+        MatOp B[2] = {op_n(T1, m), op_n(T3, m)};
+        auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T2 : Dl)[i * m + j] = v; };
+        eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
+      }
+      team.sync();
+      {
+        MatOp A[1] = {op_n(T2, m)};
+        MatOp B[1] = {op_n(V, m)};
+        auto epi = store_to(T1);
+        eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+      }
+      team.sync();
     }
-    team.sync();
-    {
-      MatOp A[1] = {op_n(T2, m)};
-      MatOp B[1] = {op_n(V, m)};
-      auto epi = store_to(T1);
-      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
-    }
-    team.sync();
     // Skew parts are exactly antisymmetric ((x - y)/2 vs (y - x)/2), which every
     // later pass relies on: precondition(r) = r / den and skew(w + t d) = w + t d
     // hold bit for bit for exactly skew r, w, d.
+    const bool approx = a.approx_basis != 0;
     SSN_FOR_IJ(team, m, {
       const int et = j * m + i;
       Ce[e] = (T1[e] - T1[et]) / 2;
@@ -229,7 +298,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       Wm[e] = 0.0;
       Pm[e] = (i == j) ? 1.0 : 0.0;
       Qm[e] = 0.0;
-      Sr[e] = (i == j) ? lam[i] : 0.0;
+      if (!approx) Sr[e] = (i == j) ? lam[i] : 0.0;
     })
     team.sync();
 
@@ -248,7 +317,13 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
         }
         team.sync();
         // sandwich (:67-71): Yr = P diag(l) - Q Ce, Yi = P Ce + Q diag(l)
-        {
+        if (approx) {
+          // full rotated Gram: Yr + i Yi = (P + iQ)(CrE + i Ce)
+          MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
+          MatOp B[2] = {op_n(CrE, m), op_n(Ce, m)};
+          auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T2)[i * m + j] = v; };
+          eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
+        } else {
           MatOp A[2] = {op_n(Qm, m), op_n(Pm, m)};
           MatOp B[1] = {op_n(Ce, m)};
           auto epi = [&](int o, int i, int j, double v) {

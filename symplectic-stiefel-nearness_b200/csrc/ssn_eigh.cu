@@ -37,16 +37,32 @@ __device__ __forceinline__ int rr_index(int slot, int st, int m1) {
 // t = sgn(h) g / (|h| + hypot(h, g)) with h = aqq - app, g = 2 a_pq (the
 // smaller root of t^2 + 2 (h/g) t - 1 = 0), c = 1/sqrt(1 + t^2), s = t c.
 // Skipped (identity) when a_pq^2 <= eps^2 |a_pp a_qq|.
-__device__ __forceinline__ bool make_rotation(double app, double aqq, double apq, double& c, double& s,
-                                              double& t) {
-  c = 1.0;
-  s = 0.0;
-  t = 0.0;
-  if (!(apq * apq > (DBL_EPSILON * DBL_EPSILON) * fabs(app * aqq))) return false;
-  const double h = aqq - app, g = 2.0 * apq;
-  const double r = sqrt(h * h + g * g);
-  t = (h >= 0.0 ? g : -g) / (fabs(h) + r);
-  c = rsqrt(1.0 + t * t);
+template <class Real>
+struct JReal;
+template <>
+struct JReal<double> {
+  using V2 = double2;
+  static constexpr double eps = DBL_EPSILON;
+  __device__ static double2 make2(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct JReal<float> {
+  using V2 = float2;
+  static constexpr float eps = FLT_EPSILON;
+  __device__ static float2 make2(float a, float b) { return make_float2(a, b); }
+};
+
+template <class Real>
+__device__ __forceinline__ bool make_rotation(Real app, Real aqq, Real apq, Real& c, Real& s, Real& t) {
+  constexpr Real eps = JReal<Real>::eps;
+  c = Real(1);
+  s = Real(0);
+  t = Real(0);
+  if (!(apq * apq > (eps * eps) * fabs(app * aqq))) return false;
+  const Real h = aqq - app, g = Real(2) * apq;
+  const Real r = sqrt(h * h + g * g);
+  t = (h >= Real(0) ? g : -g) / (fabs(h) + r);
+  c = rsqrt(Real(1) + t * t);
   s = t * c;
   return true;
 }
@@ -78,18 +94,22 @@ __device__ __forceinline__ void host_block(int ap, int m, int& bx, int& by, int&
   by = pair_of_slot(sy, m);
 }
 
+template <class Real>
 __global__ void __launch_bounds__(kJacobiThreads, 1)
     jacobi_values_kernel(const double* __restrict__ Cr, double* __restrict__ values,
                          double* __restrict__ scale_out, int32_t* __restrict__ sweeps_out,
-                         int32_t* __restrict__ status_out, double* __restrict__ rlog,
-                         int32_t* __restrict__ nsteps_out, int32_t* __restrict__ order_out, int m) {
-  extern __shared__ __align__(16) double sm[];
+                         int32_t* __restrict__ status_out, Real* __restrict__ rlog,
+                         int32_t* __restrict__ nsteps_out, int32_t* __restrict__ order_out, int m,
+                         int max_sweeps, int strict) {
+  using V2 = typename JReal<Real>::V2;
+  extern __shared__ __align__(16) double sm_raw[];
+  Real* sm = reinterpret_cast<Real*>(sm_raw);
   const int inst = blockIdx.x, tid = threadIdx.x;
   const int ld = m + 1, M = m / 2, m1 = m - 1;
-  double* A = sm;                                                    // m x ld
-  double2* cs = reinterpret_cast<double2*>(A + ((m * ld + 1) & ~1)); // [2][64]: (c, s)
-  double2* dg = cs + 2 * 64;                                         // [2][64]: diagonal entries after the rotation
-  double* tt = reinterpret_cast<double*>(dg + 2 * 64);               // [2][64]: tan
+  Real* A = sm;                                                      // m x ld
+  V2* cs = reinterpret_cast<V2*>(A + ((m * ld + 3) & ~3));           // [2][64]: (c, s)
+  V2* dg = cs + 2 * 64;                                              // [2][64]: diagonal entries after the rotation
+  Real* tt = reinterpret_cast<Real*>(dg + 2 * 64);                   // [2][64]: tan
   int2* pq = reinterpret_cast<int2*>(tt + 2 * 64);                   // [2][64]: (p, q), p < q
   double* red = reinterpret_cast<double*>(pq + 2 * 64);              // kJacobiThreads/32
   int* ctl = reinterpret_cast<int*>(red + kJacobiThreads / 32);      // [0..1]: rotated in sweep (parity), [2]: last step+1
@@ -101,14 +121,14 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   constexpr int kHostFlag = 0x100;
 
   const double* C = Cr + (size_t)inst * m * m;
-  double* L = rlog + (size_t)inst * kMaxSweeps * m1 * M * 2;
+  Real* L = rlog + (size_t)inst * kMaxSweeps * m1 * M * 2;
   double tr = 0.0;
   for (int i = tid; i < m; i += kJacobiThreads) tr += C[(size_t)i * m + i];
   tr = block_sum<kJacobiThreads>(tr, red);
   const double scale = fmax(tr / m, 1.0);
   for (int e = tid; e < m * m; e += kJacobiThreads) {
     const int i = e / m, j = e - i * m;
-    A[i * ld + j] = C[e] / scale;
+    A[i * ld + j] = static_cast<Real>(C[e] / scale);
   }
   // block list: off-diagonal blocks (a < b) row-major, then the diagonal blocks.
   // Host blocks carry kHostFlag in .y and are skipped by the generic threads.
@@ -135,11 +155,11 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   if (tid == 0) { ctl[0] = 0; ctl[1] = 0; ctl[2] = 0; ctl[3] = 0; }
   __syncthreads();
 
-  auto rotate_pair = [&](int a, int st, int buf, int g, double app, double aqq, double apq, int p, int q) {
-    double c, s, t;
-    const bool rot = make_rotation(app, aqq, apq, c, s, t);
-    cs[buf * 64 + a] = make_double2(c, s);
-    dg[buf * 64 + a] = make_double2(app - t * apq, aqq + t * apq);
+  auto rotate_pair = [&](int a, int st, int buf, int g, Real app, Real aqq, Real apq, int p, int q) {
+    Real c, s, t;
+    const bool rot = make_rotation<Real>(app, aqq, apq, c, s, t);
+    cs[buf * 64 + a] = JReal<Real>::make2(c, s);
+    dg[buf * 64 + a] = JReal<Real>::make2(app - t * apq, aqq + t * apq);
     tt[buf * 64 + a] = t;
     pq[buf * 64 + a] = make_int2(p, q);
     L[((size_t)g * M + a) * 2 + 0] = c;
@@ -160,12 +180,12 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
 
   int g = 0, st = 0, sweep = 0;
   bool converged = false;
-  const int max_steps = kMaxSweeps * m1;
+  const int max_steps = imin(max_sweeps, kMaxSweeps) * m1;
   while (g < max_steps) {
     const int cur = g & 1, nxt = cur ^ 1;
     const int nsweep = (st + 1 == m1) ? sweep + 1 : sweep;
-    const double2* csc = cs + cur * 64;
-    const double2* dgc = dg + cur * 64;
+    const V2* csc = cs + cur * 64;
+    const V2* dgc = dg + cur * 64;
     const int2* pqc = pq + cur * 64;
     if (hosted && tid < kHostThreads) {
       const int ap = tid;
@@ -173,16 +193,16 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
         int bx, by, sx, sy;
         host_block(ap, m, bx, by, sx, sy);
         const int x = rr_index(sx, st, m1), y = rr_index(sy, st, m1);   // next pair's indices
-        const double2 ra = csc[bx], rb = csc[by];
+        const V2 ra = csc[bx], rb = csc[by];
         const int2 ia = pqc[bx], ib = pqc[by];
-        double nv[2][2];
+        Real nv[2][2];
         nv[0][0] = A[ia.x * ld + ib.x];
         nv[0][1] = A[ia.x * ld + ib.y];
         nv[1][0] = A[ia.y * ld + ib.x];
         nv[1][1] = A[ia.y * ld + ib.y];
-        if (ra.y != 0.0 || rb.y != 0.0) {
-          const double u0 = ra.x * nv[0][0] - ra.y * nv[1][0], u1 = ra.x * nv[0][1] - ra.y * nv[1][1];
-          const double v0 = ra.y * nv[0][0] + ra.x * nv[1][0], v1 = ra.y * nv[0][1] + ra.x * nv[1][1];
+        if (ra.y != Real(0) || rb.y != Real(0)) {
+          const Real u0 = ra.x * nv[0][0] - ra.y * nv[1][0], u1 = ra.x * nv[0][1] - ra.y * nv[1][1];
+          const Real v0 = ra.y * nv[0][0] + ra.x * nv[1][0], v1 = ra.y * nv[0][1] + ra.x * nv[1][1];
           nv[0][0] = u0 * rb.x - u1 * rb.y;
           nv[0][1] = u0 * rb.y + u1 * rb.x;
           nv[1][0] = v0 * rb.x - v1 * rb.y;
@@ -198,9 +218,9 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
         }
         // x belongs to pair bx, y to pair by; their diagonal entries after this step
         const int ux = (x == ia.x) ? 0 : 1, uy = (y == ib.x) ? 0 : 1;
-        const double dx = ux == 0 ? dgc[bx].x : dgc[bx].y;
-        const double dy = uy == 0 ? dgc[by].x : dgc[by].y;
-        const double axy = nv[ux][uy];
+        const Real dx = ux == 0 ? dgc[bx].x : dgc[bx].y;
+        const Real dy = uy == 0 ? dgc[by].x : dgc[by].y;
+        const Real axy = nv[ux][uy];
         const bool xfirst = x < y;
         if (rotate_pair(ap, 0, nxt, g + 1, xfirst ? dx : dy, xfirst ? dy : dx, axy, xfirst ? x : y,
                         xfirst ? y : x)) {
@@ -214,26 +234,26 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
       for (int k = first; k < nblk; k += stride) {
         const short2 ab = blk[k];
         if (ab.y & kHostFlag) continue;          // owned by a host thread
-        const double2 ra = csc[ab.x];
+        const V2 ra = csc[ab.x];
         if (ab.x == ab.y) {                      // diagonal block of pair a
-          if (ra.y == 0.0) continue;
+          if (ra.y == Real(0)) continue;
           const int2 ia = pqc[ab.x];
-          const double2 d = dgc[ab.x];
+          const V2 d = dgc[ab.x];
           A[ia.x * ld + ia.x] = d.x;
           A[ia.y * ld + ia.y] = d.y;
-          A[ia.x * ld + ia.y] = 0.0;
-          A[ia.y * ld + ia.x] = 0.0;
+          A[ia.x * ld + ia.y] = Real(0);
+          A[ia.y * ld + ia.x] = Real(0);
           continue;
         }
-        const double2 rb = csc[ab.y];
-        if (ra.y == 0.0 && rb.y == 0.0) continue;
+        const V2 rb = csc[ab.y];
+        if (ra.y == Real(0) && rb.y == Real(0)) continue;
         const int2 ia = pqc[ab.x], ib = pqc[ab.y];
-        const double x = A[ia.x * ld + ib.x], y = A[ia.x * ld + ib.y];
-        const double z = A[ia.y * ld + ib.x], w = A[ia.y * ld + ib.y];
-        const double u0 = ra.x * x - ra.y * z, u1 = ra.x * y - ra.y * w;   // rows of J_a^T M
-        const double v0 = ra.y * x + ra.x * z, v1 = ra.y * y + ra.x * w;
-        const double n00 = u0 * rb.x - u1 * rb.y, n01 = u0 * rb.y + u1 * rb.x;
-        const double n10 = v0 * rb.x - v1 * rb.y, n11 = v0 * rb.y + v1 * rb.x;
+        const Real x = A[ia.x * ld + ib.x], y = A[ia.x * ld + ib.y];
+        const Real z = A[ia.y * ld + ib.x], w = A[ia.y * ld + ib.y];
+        const Real u0 = ra.x * x - ra.y * z, u1 = ra.x * y - ra.y * w;   // rows of J_a^T M
+        const Real v0 = ra.y * x + ra.x * z, v1 = ra.y * y + ra.x * w;
+        const Real n00 = u0 * rb.x - u1 * rb.y, n01 = u0 * rb.y + u1 * rb.x;
+        const Real n10 = v0 * rb.x - v1 * rb.y, n11 = v0 * rb.y + v1 * rb.x;
         A[ia.x * ld + ib.x] = n00;
         A[ib.x * ld + ia.x] = n00;
         A[ia.x * ld + ib.y] = n01;
@@ -275,10 +295,10 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
 
   // eigenvalues in ascending order; ties by index
   for (int i = tid; i < m; i += kJacobiThreads) {
-    const double li = A[i * ld + i];
+    const Real li = A[i * ld + i];
     int r = 0;
     for (int j = 0; j < m; ++j) {
-      const double lj = A[j * ld + j];
+      const Real lj = A[j * ld + j];
       r += (lj < li || (lj == li && j < i)) ? 1 : 0;
     }
     values[(size_t)inst * m + r] = li;
@@ -291,7 +311,8 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
     bool finite = true;
     for (int i = 0; i < m; ++i) finite = finite && isfinite(A[i * ld + i]);
     if (status_out)
-      status_out[inst] = !finite ? SSN_INSTANCE_NONFINITE : (converged ? SSN_INSTANCE_CONVERGED : SSN_INSTANCE_EIGH);
+      status_out[inst] = !finite ? SSN_INSTANCE_NONFINITE
+                         : (converged || !strict) ? SSN_INSTANCE_CONVERGED : SSN_INSTANCE_EIGH;
   }
 }
 
@@ -302,15 +323,18 @@ constexpr int kVecChunk = 16;   // log steps staged in shared memory at a time
 // keeps the pair table of all m - 1 steps of a sweep and stages the rotation
 // log through shared memory in chunks of kVecChunk steps.  Columns are written
 // in ascending eigenvalue order.
+template <class Real>
 __global__ void __launch_bounds__(kVecWarps * 32)
-    jacobi_vectors_kernel(const double* __restrict__ rlog, const int32_t* __restrict__ nsteps,
+    jacobi_vectors_kernel(const Real* __restrict__ rlog, const int32_t* __restrict__ nsteps,
                           const int32_t* __restrict__ order, double* __restrict__ vectors, int m) {
-  extern __shared__ __align__(16) double sv[];
+  using V2 = typename JReal<Real>::V2;
+  extern __shared__ __align__(16) double sv_raw[];
+  Real* sv = reinterpret_cast<Real*>(sv_raw);
   const int inst = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * kVecWarps + warp;
   const int M = m / 2, m1 = m - 1, ld = m + 1;
-  double2* chunk = reinterpret_cast<double2*>(sv);                    // [kVecChunk][M]
-  double* v = sv + 2 * kVecChunk * M + warp * ld;
+  V2* chunk = reinterpret_cast<V2*>(sv);                              // [kVecChunk][M]
+  Real* v = sv + 2 * kVecChunk * M + warp * ld;
   short2* pt = reinterpret_cast<short2*>(sv + 2 * kVecChunk * M + kVecWarps * ld);  // [m1][M]
   for (int e = threadIdx.x; e < m1 * M; e += kVecWarps * 32) {
     const int st = e / M, a = e - st * M;
@@ -320,8 +344,8 @@ __global__ void __launch_bounds__(kVecWarps * 32)
   }
   const bool active = row < m;
   if (active)
-    for (int c = lane; c < m; c += 32) v[c] = (c == row) ? 1.0 : 0.0;
-  const double2* L = reinterpret_cast<const double2*>(rlog + (size_t)inst * kMaxSweeps * m1 * M * 2);
+    for (int c = lane; c < m; c += 32) v[c] = (c == row) ? Real(1) : Real(0);
+  const V2* L = reinterpret_cast<const V2*>(rlog + (size_t)inst * kMaxSweeps * m1 * M * 2);
   const int n = nsteps[inst];
   int st = 0;
   for (int g0 = 0; g0 < n; g0 += kVecChunk) {
@@ -331,13 +355,13 @@ __global__ void __launch_bounds__(kVecWarps * 32)
     __syncthreads();
     if (active) {
       for (int gg = 0; gg < cnt; ++gg) {
-        const double2* cr = chunk + gg * M;
+        const V2* cr = chunk + gg * M;
         const short2* pr = pt + st * M;
         for (int a = lane; a < M; a += 32) {
-          const double2 r = cr[a];
-          if (r.y == 0.0) continue;
+          const V2 r = cr[a];
+          if (r.y == Real(0)) continue;
           const short2 ij = pr[a];
-          const double vp = v[ij.x], vq = v[ij.y];
+          const Real vp = v[ij.x], vq = v[ij.y];
           v[ij.x] = r.x * vp - r.y * vq;
           v[ij.y] = r.y * vp + r.x * vq;
         }
@@ -352,39 +376,61 @@ __global__ void __launch_bounds__(kVecWarps * 32)
   for (int c = lane; c < m; c += 32) out[ord[c]] = v[c];
 }
 
-size_t eigh_smem_bytes(int m) {
+template <class Real>
+static size_t eigh_smem_bytes_t(int m) {
   const int M = m / 2;
-  return sizeof(double) * ((size_t)((m * (m + 1) + 1) & ~1)) + sizeof(double2) * 4 * 64 +
-         sizeof(double) * 2 * 64 + sizeof(int2) * 2 * 64 + sizeof(double) * (kJacobiThreads / 32) +
+  return sizeof(Real) * ((size_t)((m * (m + 1) + 3) & ~3)) + 2 * sizeof(Real) * 4 * 64 +
+         sizeof(Real) * 2 * 64 + sizeof(int2) * 2 * 64 + sizeof(double) * (kJacobiThreads / 32) +
          sizeof(int) * 4 + sizeof(short2) * (size_t)(M * (M + 1) / 2 + 1) + 16;
 }
+
+size_t eigh_smem_bytes(int m) { return eigh_smem_bytes_t<double>(m); }
 
 size_t eigh_workspace_bytes(int batch, int m) {
   return sizeof(double) * eigh_log_doubles(batch, m) + sizeof(int32_t) * (size_t)batch * (m + 1) + 256;
 }
 
-cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, double* scale,
-                        int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
-                        cudaStream_t stream) {
-  double* rlog = static_cast<double*>(workspace);
-  int32_t* nsteps = reinterpret_cast<int32_t*>(rlog + eigh_log_doubles(batch, m));
+template <class Real>
+static cudaError_t launch_eigh_t(const double* Cr, double* values, double* vectors, double* scale,
+                                 int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
+                                 int max_sweeps, bool strict, cudaStream_t stream) {
+  Real* rlog = static_cast<Real*>(workspace);
+  int32_t* nsteps = reinterpret_cast<int32_t*>(static_cast<double*>(workspace) + eigh_log_doubles(batch, m));
   int32_t* order = nsteps + batch;
-  const size_t smem = eigh_smem_bytes(m);
-  cudaError_t err = cudaFuncSetAttribute(jacobi_values_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const size_t smem = eigh_smem_bytes_t<Real>(m);
+  cudaError_t err = cudaFuncSetAttribute(jacobi_values_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;
-  jacobi_values_kernel<<<batch, kJacobiThreads, smem, stream>>>(Cr, values, scale, sweeps, status, rlog,
-                                                               nsteps, order, m);
+  jacobi_values_kernel<Real><<<batch, kJacobiThreads, smem, stream>>>(Cr, values, scale, sweeps, status, rlog,
+                                                                     nsteps, order, m, max_sweeps, strict ? 1 : 0);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
-  const size_t vsmem = sizeof(double) * (2 * kVecChunk * (m / 2) + kVecWarps * (m + 1)) +
+  const size_t vsmem = sizeof(Real) * (2 * kVecChunk * (m / 2) + kVecWarps * (m + 1)) +
                        sizeof(short2) * (size_t)(m - 1) * (m / 2) + 16;
-  err = cudaFuncSetAttribute(jacobi_vectors_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  err = cudaFuncSetAttribute(jacobi_vectors_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(vsmem));
   if (err != cudaSuccess) return err;
   dim3 grid(cdiv(m, kVecWarps), batch);
-  jacobi_vectors_kernel<<<grid, kVecWarps * 32, vsmem, stream>>>(rlog, nsteps, order, vectors, m);
+  jacobi_vectors_kernel<Real><<<grid, kVecWarps * 32, vsmem, stream>>>(rlog, nsteps, order, vectors, m);
   return cudaGetLastError();
+}
+
+cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, double* scale,
+                        int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
+                        cudaStream_t stream) {
+  return launch_eigh_t<double>(Cr, values, vectors, scale, sweeps, status, batch, m, workspace, kMaxSweeps,
+                               true, stream);
+}
+
+cudaError_t launch_eigh_approx(const double* Cr, double* values, double* vectors, double* scale,
+                               int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
+                               int max_sweeps, bool fp32, cudaStream_t stream) {
+  if (max_sweeps < 1) max_sweeps = 1;
+  if (max_sweeps > kMaxSweeps) max_sweeps = kMaxSweeps;
+  return fp32 ? launch_eigh_t<float>(Cr, values, vectors, scale, sweeps, status, batch, m, workspace,
+                                     max_sweeps, false, stream)
+              : launch_eigh_t<double>(Cr, values, vectors, scale, sweeps, status, batch, m, workspace,
+                                      max_sweeps, false, stream);
 }
 
 }  // namespace ssn

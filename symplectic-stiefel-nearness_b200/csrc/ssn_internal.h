@@ -29,6 +29,13 @@ struct DualArgs {
   int64_t* iterations;     // [B] out
   int32_t* status;         // [B] out
   int32_t* counters;       // [B,4] out: newton steps, hvps, trials, fallbacks (may be null)
+  // Approximate eigenbasis (split-precision form): the vectors only roughly
+  // diagonalise Cr/s.  The kernel then works with the full rotated Gram
+  // V^T (Cr/s) V in the sandwich and takes the preconditioner's lambda from its
+  // diagonal.  orthogonalize: first make V orthogonal to FP64 rounding with two
+  // Newton-Schulz steps V <- V (3I - V^T V) / 2 (vectors from FP32 rotations).
+  int approx_basis;
+  int orthogonalize;
 };
 
 size_t eigh_smem_bytes(int m);
@@ -36,6 +43,11 @@ size_t eigh_workspace_bytes(int batch, int m);
 cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, double* scale,
                         int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
                         cudaStream_t stream);
+// Jacobi capped at max_sweeps (no convergence requirement), FP32 or FP64 rotations:
+// the rough eigenbasis of the split-precision form.
+cudaError_t launch_eigh_approx(const double* Cr, double* values, double* vectors, double* scale,
+                               int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
+                               int max_sweeps, bool fp32, cudaStream_t stream);
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
 cudaError_t launch_probe_fp64_mma(double* sink, int iters, double* flops, cudaStream_t stream);
 cudaError_t launch_probe_s8_mma(const int8_t* A, const int8_t* B, int32_t* C, int n, int k, int* stall,

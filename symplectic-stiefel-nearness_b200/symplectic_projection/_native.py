@@ -32,11 +32,11 @@ PROTOTYPES = {
     "ssn_gram_noalloc": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P]),
     "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P]),
     "ssn_eigh_workspace_bytes": (_SZ, [_I, _I]),
-    "ssn_eigh": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
+    "ssn_eigh": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
     "ssn_dual_workspace_bytes": (_SZ, [_I, _I]),
     "ssn_dual": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
     "ssn_newton_workspace_bytes": (_SZ, [_I, _I]),
-    "ssn_newton": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
+    "ssn_newton": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
     "ssn_probe_fp64_mma": (_I, [_P, _I, _P, _P]),
     "ssn_probe_s8_mma": (_I, [_P, _P, _P, _I, _I, _P, _P]),
     "ssn_inner_products": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
@@ -59,7 +59,12 @@ class Options(ctypes.Structure):
     """ssn_options (include/ssn.h)."""
     _fields_ = [("max_newton", ctypes.c_int), ("max_cg", ctypes.c_int),
                 ("max_backtrack", ctypes.c_int), ("feas_tol", ctypes.c_double),
-                ("reserved", ctypes.c_int * 8)]
+                ("precision", ctypes.c_int), ("eig_sweeps", ctypes.c_int),
+                ("reserved", ctypes.c_int * 6)]
+
+
+# ssn_options.precision values (include/ssn.h)
+PRECISIONS = {"fp64": 0, "split": 1}
 
 
 _lib = None
@@ -82,10 +87,14 @@ def load() -> ctypes.CDLL:
     return _lib
 
 
-def options(max_newton=100, max_cg=150, max_backtrack=40, feas_tol=1e-8) -> Options:
+def options(max_newton=100, max_cg=150, max_backtrack=40, feas_tol=1e-8, precision="fp64",
+            eig_sweeps=0) -> Options:
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     opt = Options()
     load().ssn_default_options(ctypes.byref(opt))
     opt.max_newton, opt.max_cg, opt.max_backtrack, opt.feas_tol = max_newton, max_cg, max_backtrack, feas_tol
+    opt.precision, opt.eig_sweeps = PRECISIONS[precision], eig_sweeps
     return opt
 
 

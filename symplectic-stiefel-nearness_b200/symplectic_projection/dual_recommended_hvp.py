@@ -62,8 +62,15 @@ def _pinned_like(T: torch.Tensor) -> torch.Tensor:
 @torch.no_grad()
 def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
              max_backtrack: int = MAX_BACKTRACK, feas_tol: float = FEAS_TOL,
+             precision: str = "fp64", eig_sweeps: int = 0,
              raise_on_failure: bool = False) -> SolveResult:
-    """Device-resident solve with per-instance status.  T must be a CUDA tensor."""
+    """Device-resident solve with per-instance status.  T must be a CUDA tensor.
+
+    precision="fp64" is the plain FP64 form (the reference's iterates);
+    precision="split" takes the eigenbasis from ``eig_sweeps`` FP32 Jacobi
+    sweeps (0: the library default) and works with the full rotated Gram, so
+    it reaches the same dual optimum under the same acceptance bounds.
+    """
     batch, n, m = _check_target(T)
     dev = N.require_cuda_f64(T)
     T = T.contiguous()
@@ -76,7 +83,7 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
     lib = N.load()
     nbytes = lib.ssn_workspace_bytes(batch, n, m)
     ws = workspace(dev, nbytes)
-    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol)
+    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps)
     N.check(lib.ssn_solve(T.data_ptr(), X.data_ptr(), omega.data_ptr(), iterations.data_ptr(),
                           status.data_ptr(), batch, n, m, ws.data_ptr(), nbytes,
                           N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_solve")
@@ -205,10 +212,12 @@ def gram_chunks(T, blocks=None):
 
 
 @torch.no_grad()
-def eigh_scaled(Cr):
-    """(values, vectors, scale) with Cr/scale = V diag(values) V^T, scale = max(1, tr(Cr)/m).
+def eigh_scaled(Cr, precision="fp64", eig_sweeps=0):
+    """(values, vectors, scale, sweeps) with Cr/scale = V diag(values) V^T, scale = max(1, tr(Cr)/m).
 
     Device Jacobi replacing torch.linalg.eigh at dual_recommended_hvp.py:106-108.
+    precision="split" returns the rough basis of the split-precision form
+    (``eig_sweeps`` FP32 sweeps; V only approximately diagonalises Cr/scale).
     """
     dev = N.require_cuda_f64(Cr)
     batch, m, _ = Cr.shape
@@ -220,8 +229,10 @@ def eigh_scaled(Cr):
     lib = N.load()
     nbytes = lib.ssn_eigh_workspace_bytes(batch, m)
     ws = workspace(dev, nbytes)
+    opt = N.options(precision=precision, eig_sweeps=eig_sweeps)
     N.check(lib.ssn_eigh(Cr.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(),
-                         sweeps.data_ptr(), batch, m, ws.data_ptr(), nbytes, N.stream_handle(dev)), "ssn_eigh")
+                         sweeps.data_ptr(), batch, m, ws.data_ptr(), nbytes, N.ctypes.byref(opt),
+                         N.stream_handle(dev)), "ssn_eigh")
     return values, vectors, scale, sweeps
 
 
@@ -245,7 +256,8 @@ def dual_batch(Cr, Ci, final=None, **options):
     nbytes = lib.ssn_dual_workspace_bytes(batch, m)
     ws = workspace(dev, nbytes)
     opt = N.options(options.get("max_newton", MAX_NEWTON), options.get("max_cg", MAX_CG),
-                    options.get("max_backtrack", MAX_BACKTRACK), options.get("feas_tol", FEAS_TOL))
+                    options.get("max_backtrack", MAX_BACKTRACK), options.get("feas_tol", FEAS_TOL),
+                    options.get("precision", "fp64"), options.get("eig_sweeps", 0))
     N.check(lib.ssn_dual(Cr.data_ptr(), Ci.data_ptr(), omega.data_ptr(), P.data_ptr(), Q.data_ptr(),
                          iterations.data_ptr(), status.data_ptr(), batch, m, ws.data_ptr(), nbytes,
                          N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_dual")
