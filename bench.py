@@ -218,7 +218,7 @@ def run_ours(args):
     def phases(opt, ev=None):
         if ev: ev[0].record(stream)
         N.check(lib.ssn_gram(A_ptr, D_ptr, stride, Cr.data_ptr(), Ci.data_ptr(), B, n, m,
-                             ws.data_ptr(), gram_bytes, sh), "gram")
+                             ws.data_ptr(), gram_bytes, N.ctypes.byref(opt), sh), "gram")
         if ev: ev[1].record(stream)
         N.check(lib.ssn_eigh(Cr.data_ptr(), values.data_ptr(), vectors.data_ptr(), scale.data_ptr(),
                              sweeps.data_ptr(), B, m, ws.data_ptr(), eigh_bytes, N.ctypes.byref(opt), sh), "eigh")

@@ -109,11 +109,16 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations,
  * strides ab_stride (elements, >= rows*m).  Replaces gram_add_
  * (gram_triangle_reflect.py:19-36; kernels gram_offdiag / gram_diagonal,
  * gram_triangle_reflect.cu:51-104).  Needs ssn_gram_workspace_bytes bytes.
+ * opt NULL or SSN_PRECISION_FP64: FP64 tensor-core (DMMA) products.
+ * SSN_PRECISION_SPLIT: INT8 Ozaki products on the tcgen05 tensor cores (six
+ * balanced 8-bit digits per value with per-(row chunk, column) power-of-two
+ * scales, exact INT32 accumulation, FP64 recombination): relative error about
+ * 1e-12 of max|T|^2 per entry for Gaussian T.
  */
 size_t ssn_gram_workspace_bytes(int batch, int rows, int m);
 int ssn_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
              int batch, int rows, int m, void* workspace, size_t workspace_bytes,
-             ssn_stream_t stream);
+             const ssn_options* opt, ssn_stream_t stream);
 
 /*
  * ssn_gram without a workspace argument, for callers that cannot allocate

@@ -24,7 +24,7 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Workspace layout of ssn_solve (byte offsets, 256-byte aligned sections).
 struct SolveLayout {
-  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, eig_ws, total;
+  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, eig_ws, row_exp, stall, total;
 };
 
 SolveLayout solve_layout(int batch, int n, int m) {
@@ -45,10 +45,14 @@ SolveLayout solve_layout(int batch, int n, int m) {
   L.qfin = take(sizeof(double) * batch * mm);
   // the Gram partial sums share the Newton workspace (they are dead before it is used)
   const size_t work = sizeof(double) * (size_t)batch * kDualMats * mm;
-  const size_t partial = sizeof(double) * gram_partial_doubles(batch, n, m);
+  size_t partial = sizeof(double) * gram_partial_doubles(batch, n, m);
+  const size_t oz = ozaki_gram_workspace_bytes(batch, n, m);
+  if (oz > partial) partial = oz;
   L.work = take(work > partial ? work : partial);
   L.eig_status = take(sizeof(int32_t) * batch);
   L.eig_ws = take(eigh_workspace_bytes(batch, m));
+  L.row_exp = take(sizeof(int32_t) * (size_t)batch * n);     // split form: per-row scales of [A_r | D_r]
+  L.stall = take(sizeof(int32_t) * 4);                        // split form: tensor-core wait-limit flag
   L.total = off;
   return L;
 }
@@ -170,7 +174,10 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
   const int64_t stride = 2LL * n * m;
   const double* A = T;
   const double* D = T + (size_t)n * m;
-  cudaError_t e = launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
+  int32_t* row_exp = reinterpret_cast<int32_t*>(ws + L.row_exp);
+  int* stall = reinterpret_cast<int*>(ws + L.stall);
+  cudaError_t e = split_form(opt) ? launch_gram_ozaki(A, D, stride, Cr, Ci, batch, n, m, work, row_exp, stall, stream)
+                                  : launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   e = eigenbasis(opt, Cr, values, vectors, scale, nullptr, eig_status, batch, m, ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
@@ -196,21 +203,30 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
   return cuda_status(e);
 }
 
+size_t gram_fp64_bytes(int batch, int rows, int m) { return sizeof(double) * gram_partial_doubles(batch, rows, m); }
+
 size_t ssn_gram_workspace_bytes(int batch, int rows, int m) {
   if (!shape_ok(batch, m) || rows < 1) return 0;
-  return sizeof(double) * gram_partial_doubles(batch, rows, m);
+  const size_t f = gram_fp64_bytes(batch, rows, m);
+  const size_t z = align_up(ozaki_gram_workspace_bytes(batch, rows, m), 256) + 256;   // + stall flag
+  return f > z ? f : z;
 }
 
 int ssn_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci, int batch,
-             int rows, int m, void* workspace, size_t workspace_bytes, ssn_stream_t stream) {
+             int rows, int m, void* workspace, size_t workspace_bytes, const ssn_options* opt,
+             ssn_stream_t stream) {
   if (!shape_ok(batch, m) || rows < 1 || !A || !D || !Cr || !Ci || ab_stride < (int64_t)rows * m ||
-      (ab_stride % 2) != 0 || !aligned16(A) || !aligned16(D))
+      (ab_stride % 2) != 0 || !aligned16(A) || !aligned16(D) || !options_ok(opt))
     return SSN_ERR_INVALID_ARGUMENT;
   if (!workspace || workspace_bytes < ssn_gram_workspace_bytes(batch, rows, m) || !aligned16(workspace))
     return SSN_ERR_WORKSPACE;
-  return cuda_status(launch_gram(A, D, ab_stride, Cr, Ci, batch, rows, m,
-                                 static_cast<double*>(workspace),
-                                 reinterpret_cast<cudaStream_t>(stream)));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (split_form(opt)) {
+    int* stall = reinterpret_cast<int*>(static_cast<char*>(workspace) +
+                                        align_up(ozaki_gram_workspace_bytes(batch, rows, m), 256));
+    return cuda_status(launch_gram_ozaki(A, D, ab_stride, Cr, Ci, batch, rows, m, workspace, nullptr, stall, st));
+  }
+  return cuda_status(launch_gram(A, D, ab_stride, Cr, Ci, batch, rows, m, static_cast<double*>(workspace), st));
 }
 
 int ssn_recover(const double* A, const double* D, int64_t ab_stride, const double* P, const double* Q,

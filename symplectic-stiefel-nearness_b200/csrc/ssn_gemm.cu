@@ -109,6 +109,12 @@ __global__ void gram_finalize_kernel(const double* __restrict__ partial, double*
 
 int gram_splits(int batch, int rows, int max_splits) { return gram_split(batch, rows, max_splits).splits; }
 
+cudaError_t launch_gram_finalize(const double* partial, double* Cr, double* Ci, int batch, int m, int splits,
+                                 cudaStream_t stream) {
+  gram_finalize_kernel<<<dim3(cdiv(m * m, 128), batch), 128, 0, stream>>>(partial, Cr, Ci, m, splits);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
                         int batch, int rows, int m, double* partial, cudaStream_t stream, int max_splits) {
   const GramSplit gs = gram_split(batch, rows, max_splits);

@@ -59,6 +59,14 @@ int gram_splits(int batch, int rows, int max_splits);
 cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
                         int batch, int rows, int m, double* partial, cudaStream_t stream,
                         int max_splits = 1 << 30);
+// Fixed-order sum of row-split partials [B][splits][2][m][m] (Cr part, G part) into Cr and Ci = G - G^T.
+cudaError_t launch_gram_finalize(const double* partial, double* Cr, double* Ci, int batch, int m, int splits,
+                                 cudaStream_t stream);
+// Split-precision (INT8 Ozaki, tcgen05) Gram.  Workspace: ozaki_gram_workspace_bytes.
+size_t ozaki_gram_workspace_bytes(int batch, int rows, int m);
+cudaError_t launch_gram_ozaki(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
+                              int batch, int rows, int m, void* workspace, int32_t* row_exp, int* stall,
+                              cudaStream_t stream);
 cudaError_t launch_recover(const double* A, const double* D, int64_t ab_stride, const double* P,
                            const double* Q, double* Ur, double* Ui, int64_t u_stride, int batch,
                            int rows, int m, cudaStream_t stream);

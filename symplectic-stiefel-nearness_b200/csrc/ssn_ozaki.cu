@@ -1,15 +1,31 @@
 // ssn_ozaki.cu -- split-precision (INT8 Ozaki) products on the tcgen05 tensor cores.
 //
 // The contraction kernels here compute FP64 products exactly enough for the
-// dual Newton solve from INT8 digit slices: every FP64 operand row (or
-// column) is scaled by a power of two and written as S signed 7-bit digits,
-// the digit products are accumulated exactly in INT32 TMEM accumulators by
-// tcgen05.mma kind::i8, and the levels s + t <= S + 1 are recombined in FP64.
+// dual Newton solve from INT8 digit slices: every FP64 operand vector is scaled
+// by a power of two and written as six balanced 8-bit digits, the digit
+// products are accumulated exactly in INT32 TMEM accumulators by tcgen05.mma
+// kind::i8, and the levels p + q <= 5 are recombined in FP64.
+//
+// Digits.  A value x of a vector with scale exponent E (|x| < 2^E for every
+// entry of the vector) is written as the integer F = rint(x 2^(46-E)),
+// |F| <= 2^46, in six balanced base-256 digits d_0 (most significant) .. d_5,
+// each in [-128, 127]: F = sum_i d_i 256^(5-i).  Balanced digits make the
+// truncation of the dropped digit products unbiased (plain unsigned low bytes
+// make every dropped product positive, and the error then grows with K).
+// One FMA does all of it: z = x * 2^(46-E) + (1.5 * 2^52 + C) with
+// C = sum_i 128 * 256^i rounds x 2^(46-E) to the integer F and leaves F + C in
+// the low 48 mantissa bits of z; byte (5-i) of F + C, XOR 0x80, is d_i.
+//
+// Products keep the digit pairs with p + q <= 5 (21 of 36), accumulated per
+// level l = p + q in its own INT32 TMEM accumulator (exact: 6 pairs x 2^14 x K
+// < 2^31 for K < 21845), and recombined in FP64 as
+//     sum_l 256^(10-l) acc_l * 2^(E_a - 46) * 2^(E_b - 46).
 //
 // This file starts with the single-CTA INT8 MMA used to check the descriptor,
 // TMEM and completion plumbing bit for bit against an integer reference.
 #include <cuda_runtime.h>
 
+#include "ssn_common.cuh"
 #include "ssn_internal.h"
 #include "ssn_tc.cuh"
 
@@ -94,6 +110,462 @@ cudaError_t launch_probe_s8_mma(const int8_t* A, const int8_t* B, int32_t* C, in
   if (err != cudaSuccess) return err;
   probe_s8_mma_kernel<<<1, kProbeThreadsS8, smem, stream>>>(A, B, C, n, k, stall);
   return cudaGetLastError();
+}
+
+// ============================================================== Ozaki digits
+namespace oz {
+
+constexpr int kDigits = 6;
+constexpr int kFrac = 8 * kDigits - 2;              // 46
+constexpr int kExpNonFinite = 4096;                 // exponent code of a vector with Inf / NaN
+constexpr int kExpMin = -960;                       // 2^(kFrac - E) stays finite
+constexpr double kMagic = 6755399441055744.0 + 141289400074368.0;   // 1.5 * 2^52 + 0x808080808080
+
+// Exponent E with max < 2^E from the bit pattern of max |x| (sign bit clear).
+__host__ __device__ __forceinline__ int exp_of_maxbits(unsigned long long bits) {
+  if (bits >= 0x7FF0000000000000ull) return kExpNonFinite;
+  if (bits == 0ull) return kExpMin;
+  const int eb = static_cast<int>(bits >> 52);
+  const int e = (eb > 0 ? eb : 1) - 1022;
+  return e < kExpMin ? kExpMin : e;
+}
+
+__device__ __forceinline__ double pow2(int e) {   // exact 2^e for -1022 <= e <= 1023
+  return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+}
+
+__device__ __forceinline__ unsigned long long abs_bits(double x) {
+  return static_cast<unsigned long long>(__double_as_longlong(x)) & 0x7FFFFFFFFFFFFFFFull;
+}
+
+// Digit words of four values sharing the scale sc = 2^(kFrac - E): w[i] holds
+// digit i of x[0..3] in bytes 0..3 (K-contiguous rows of a K-major operand).
+__device__ __forceinline__ void slice4(const double (&x)[4], double sc, uint32_t (&w)[kDigits]) {
+  uint32_t lo[4], hi[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double z = fma(x[q], sc, kMagic);
+    lo[q] = static_cast<uint32_t>(__double2loint(z));
+    hi[q] = static_cast<uint32_t>(__double2hiint(z));
+  }
+  // 4 x 4 byte transpose of lo, 4 x 2 of the low half of hi
+  const uint32_t t0 = __byte_perm(lo[0], lo[1], 0x5140), t1 = __byte_perm(lo[0], lo[1], 0x7362);
+  const uint32_t t2 = __byte_perm(lo[2], lo[3], 0x5140), t3 = __byte_perm(lo[2], lo[3], 0x7362);
+  const uint32_t t4 = __byte_perm(hi[0], hi[1], 0x5140), t5 = __byte_perm(hi[2], hi[3], 0x5140);
+  w[5] = __byte_perm(t0, t2, 0x5410) ^ 0x80808080u;   // byte 0 of F + C
+  w[4] = __byte_perm(t0, t2, 0x7632) ^ 0x80808080u;   // byte 1
+  w[3] = __byte_perm(t1, t3, 0x5410) ^ 0x80808080u;   // byte 2
+  w[2] = __byte_perm(t1, t3, 0x7632) ^ 0x80808080u;   // byte 3
+  w[1] = __byte_perm(t4, t5, 0x5410) ^ 0x80808080u;   // byte 4
+  w[0] = __byte_perm(t4, t5, 0x7632) ^ 0x80808080u;   // byte 5 (most significant digit)
+}
+
+// sum_l 256^(5-l) acc_l (Horner), the digit-level recombination before scaling.
+__device__ __forceinline__ double horner6(const uint32_t (&a)[kDigits]) {
+  double v = static_cast<double>(static_cast<int32_t>(a[0]));
+#pragma unroll
+  for (int l = 1; l < kDigits; ++l) v = fma(v, 256.0, static_cast<double>(static_cast<int32_t>(a[l])));
+  return v;
+}
+
+}  // namespace oz
+
+// ============================================================== Ozaki Gram
+//
+// Cr = A^T A + D^T D and G = A^T D over row chunks of n: one CTA per (row chunk,
+// group of 32 output columns, instance).  The MMA's M = 128 rows are the m
+// columns of T (zero-padded), N = 32 the CTA's output columns, K the rows of
+// the chunk, streamed in sub-tiles of 32 rows of A and 32 rows of D.  Every
+// sub-tile is sliced into digit planes (K-major, 64 K bytes per operand row:
+// A rows then D rows) in a 3-stage shared ring; one thread issues the 63 MMAs
+// of the sub-tile (21 digit pairs x {A^T A, D^T D, A^T D}) into 12 TMEM
+// accumulators (6 levels x {Cr, G}, 32 columns each) and commits them to the
+// stage's mbarrier, which releases the stage for the sub-tile three ahead.
+// Column scales are per (chunk, column), shared by A and D so that Cr's two
+// halves can share accumulators; a pre-pass computes them (and the per-row
+// scales the recovery uses).  Partials go to [B][chunk][2][m][m] and are summed
+// in fixed order by the FP64 Gram's finalize kernel.
+namespace {
+
+constexpr int kScaleThreads = 256;
+constexpr int kScaleRows = 64;                 // rows of A and D per pre-pass block
+
+// Pre-pass: per-(chunk, column) max |x| over the rows of A and D in the chunk (as
+// bit patterns, atomicMax into a zeroed array; max is order-independent) and
+// the per-row scale exponent of [A_r | D_r] for the recovery.
+__global__ void __launch_bounds__(kScaleThreads)
+    ozaki_scale_kernel(const double* __restrict__ A, const double* __restrict__ D, int64_t ab_stride, int rows,
+                       int m, int chunk, int nchunks, unsigned long long* __restrict__ col_bits,
+                       int32_t* __restrict__ row_exp) {
+  __shared__ unsigned long long cmax[kScaleThreads / 32][kMaxM];
+  const int b = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = blockIdx.x * kScaleRows, r1 = imin(rows, r0 + kScaleRows);
+  const double* Ab = A + (size_t)b * ab_stride;
+  const double* Db = D + (size_t)b * ab_stride;
+  unsigned long long cm[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll 2
+  for (int r = r0 + warp; r < r1; r += kScaleThreads / 32) {
+    unsigned long long rm = 0ull;
+#pragma unroll
+    for (int hh = 0; hh < 2; ++hh) {
+      const int col = 2 * lane + 64 * hh;
+      if (col < m) {
+        const double2 a = *reinterpret_cast<const double2*>(Ab + (size_t)r * m + col);
+        const double2 d = *reinterpret_cast<const double2*>(Db + (size_t)r * m + col);
+        const unsigned long long c0 = max(oz::abs_bits(a.x), oz::abs_bits(d.x));
+        const unsigned long long c1 = max(oz::abs_bits(a.y), oz::abs_bits(d.y));
+        cm[2 * hh] = max(cm[2 * hh], c0);
+        cm[2 * hh + 1] = max(cm[2 * hh + 1], c1);
+        rm = max(rm, max(c0, c1));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rm = max(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+    if (lane == 0 && row_exp) row_exp[(size_t)b * rows + r] = oz::exp_of_maxbits(rm);
+  }
+#pragma unroll
+  for (int hh = 0; hh < 2; ++hh) {
+    const int col = 2 * lane + 64 * hh;
+    if (col < m) {
+      cmax[warp][col] = cm[2 * hh];
+      cmax[warp][col + 1] = cm[2 * hh + 1];
+    }
+  }
+  __syncthreads();
+  const int c = r0 / chunk;        // pre-pass blocks never straddle a chunk (chunk % kScaleRows == 0)
+  for (int j = threadIdx.x; j < m; j += kScaleThreads) {
+    unsigned long long mx = 0ull;
+    for (int w = 0; w < kScaleThreads / 32; ++w) mx = max(mx, cmax[w][j]);
+    atomicMax(&col_bits[((size_t)b * nchunks + c) * m + j], mx);
+  }
+}
+
+// Warp roles.  All slicing warps work on every sub-tile in order, so every
+// waiter sees every phase of the mbarriers it waits on: a parity wait is only
+// unambiguous when the waiter has observed the previous phase (a consumer that
+// skipped phases could see a parity match one phase early).
+constexpr int kGSliceWarps = 8;
+constexpr int kGSlicers = kGSliceWarps * 32;
+constexpr int kGMmaWarp = kGSliceWarps;                    // warp 8: MMA issuer
+constexpr int kGLoadWarp = kGSliceWarps + 1;               // warp 9: TMA producer
+constexpr int kGThreads = kGSlicers + 64;
+constexpr int kGSub = 32;                                  // rows of A (and of D) per sub-tile
+constexpr int kGN = 32;                                    // output columns per CTA (MMA N)
+constexpr int kGM = 128;                                   // MMA M: operand rows read from a digit plane
+constexpr int kGKBytes = 2 * kGSub;                        // K bytes per operand row of one digit plane
+constexpr int kGDStages = 2;                               // digit-plane stages
+constexpr int kGFStagesMax = 3;                            // FP64 staging stages (TMA bulk copies)
+constexpr int kGSmemMax = 227 * 1024 - 2304;               // opt-in limit minus the static shared memory
+constexpr uint32_t kGTmemCols = 512;                       // 2 x 6 x 32 = 384 used
+constexpr uint32_t kGSbo = (kGKBytes / 16) * tc::kCoreBytes;   // 512: 8-row group stride
+
+// Shared-memory plan of the Gram kernel for m columns.  Digit planes are packed
+// at mp16 rows; the M = 128 rows an MMA reads from plane p may run into plane
+// p + 1 (those output rows are never read), so only the last plane is padded
+// to 128 rows.  FP64 stages hold 32 rows of A then 32 rows of D.
+struct GramSmem {
+  int plane, bstack, dstage, fstage, fstages, total;
+};
+constexpr int kGBStack = oz::kDigits * kGN * kGKBytes;    // 12288: digits 0..5 of the CTA's 32 columns
+__host__ __device__ inline GramSmem gram_smem(int m) {
+  GramSmem g;
+  const int mp16 = round_up(m, 16);
+  g.plane = mp16 * kGKBytes;
+  g.bstack = (oz::kDigits - 1) * g.plane + kGM * kGKBytes;   // B copy follows the A planes of a stage
+  g.dstage = g.bstack + kGBStack;
+  g.fstage = 2 * kGSub * m * 8;
+  g.fstages = (kGSmemMax - kGDStages * g.dstage) / g.fstage;
+  if (g.fstages > kGFStagesMax) g.fstages = kGFStagesMax;
+  g.total = kGDStages * g.dstage + g.fstages * g.fstage;
+  return g;
+}
+
+// The MMAs of one sub-tile.  For a fixed digit p of the A operand (all m columns), the
+// B operand is the stack of digits q = 0 .. 5 - p of the CTA's 32 output columns
+// (rows 32 q + jj of the B copy), so one MMA with N = (6 - p) 32 adds every pair
+// (p, q) into the level accumulators p + q, which lie at TMEM columns 32 (p + q):
+// contiguous from 32 p.  Per p: A^T A and D^T D (Cr) and A^T D (G); 18 MMAs.
+template <int P>
+struct GramStack {
+  __device__ __forceinline__ static void issue(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t plane16,
+                                               bool first_tile) {
+    constexpr int N = (oz::kDigits - P) * kGN;
+    constexpr uint32_t idesc = tc::idesc_s8(kGM, N);
+    const uint64_t da = adesc + (uint64_t)(P * plane16);
+    constexpr uint32_t col = (uint32_t)P * kGN;
+    const uint32_t acc = (!first_tile || P > 0) ? 1u : 0u;
+    tc::mma_s8(tmem + col, da, bdesc, idesc, acc);                                 // A^T A
+    tc::mma_s8(tmem + col, da + 16, bdesc + 16, idesc, 1u);                        // + D^T D (K bytes 32..63)
+    tc::mma_s8(tmem + oz::kDigits * kGN + col, da, bdesc + 16, idesc, acc);        // A^T D
+    if constexpr (P + 1 < oz::kDigits) GramStack<P + 1>::issue(tmem, adesc, bdesc, plane16, first_tile);
+  }
+};
+
+__global__ void __launch_bounds__(kGThreads, 1)
+    ozaki_gram_kernel(const double* __restrict__ A, const double* __restrict__ D, int64_t ab_stride, int rows,
+                      int m, int chunk, int nchunks, int ncg, const unsigned long long* __restrict__ col_bits,
+                      double* __restrict__ partial, int* __restrict__ stall) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ uint64_t bar_full[kGFStagesMax];     // TMA -> slicers (transaction bytes)
+  __shared__ uint64_t bar_ffree[kGFStagesMax];    // slicers -> producer: FP64 stage consumed
+  __shared__ uint64_t bar_ready[kGDStages];       // slicers -> MMA issuer: digit planes written
+  __shared__ uint64_t bar_dfree[kGDStages];       // MMA commit -> slicers: digit planes consumed
+  __shared__ uint32_t tmem_slot;
+  __shared__ int s_err;
+  __shared__ double s_sc[kMaxM];      // slicing scale 2^(46 - E_j)
+  __shared__ double s_inv[kMaxM];     // recombination scale 2^(E_j - 26)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int c = blockIdx.x / ncg, h = blockIdx.x - c * ncg, b = blockIdx.y;
+  const int r0 = c * chunk, r1 = imin(rows, r0 + chunk);
+  const int nsub = cdiv(r1 - r0, kGSub);
+  const int mp16 = round_up(m, 16);
+  const GramSmem L = gram_smem(m);
+  const double* Ab = A + (size_t)b * ab_stride;
+  const double* Db = D + (size_t)b * ab_stride;
+  uint8_t* dbase = smem;
+  uint8_t* fbase = smem + kGDStages * L.dstage;
+
+  // zero the digit stages once: rows >= mp16 of the last plane are read by the MMA, never written
+  for (int i = tid * 16; i < kGDStages * L.dstage; i += kGThreads * 16)
+    *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
+  bool bad = false;
+  if (tid < kMaxM) {
+    int e = oz::kExpMin;
+    if (tid < m) e = oz::exp_of_maxbits(col_bits[((size_t)b * nchunks + c) * m + tid]);
+    bad = e == oz::kExpNonFinite;
+    if (bad) e = 0;
+    s_sc[tid] = oz::pow2(oz::kFrac - e);
+    s_inv[tid] = oz::pow2(e - 26);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kGFStagesMax; ++s) {
+      tc::mbar_init(&bar_full[s], 1);
+      tc::mbar_init(&bar_ffree[s], kGSliceWarps);
+    }
+    for (int s = 0; s < kGDStages; ++s) {
+      tc::mbar_init(&bar_ready[s], kGSliceWarps);
+      tc::mbar_init(&bar_dfree[s], 1);
+    }
+    s_err = 0;
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_slot, kGTmemCols);
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  bad = __syncthreads_or(bad) != 0;
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+
+  if (!bad) {
+    if (warp == kGLoadWarp) {
+      // ---- TMA producer: FP64 rows of sub-tile t of A and D into FP64 stage t % fstages
+      if (lane == 0) {
+        bool ok = true;
+        for (int t = 0; t < nsub && ok; ++t) {
+          const int f = t % L.fstages;
+          if (t >= L.fstages) ok = tc::mbar_wait(&bar_ffree[f], ((t / L.fstages) - 1) & 1, tc::kWaitPolls);
+          if (!ok || *reinterpret_cast<volatile int*>(&s_err)) break;
+          const int rs = r0 + t * kGSub;
+          const uint32_t bytes = (uint32_t)(imin(kGSub, r1 - rs) * m * 8);
+          uint8_t* dst = fbase + f * L.fstage;
+          tc::mbar_arrive_expect_tx(&bar_full[f], 2 * bytes);
+          tc::bulk_g2s(dst, Ab + (size_t)rs * m, bytes, &bar_full[f]);
+          tc::bulk_g2s(dst + kGSub * m * 8, Db + (size_t)rs * m, bytes, &bar_full[f]);
+        }
+        if (!ok) atomicExch(&s_err, 1);
+      }
+    } else if (warp == kGMmaWarp) {
+      // ---- MMA issuer: the 63 MMAs of each sub-tile once its digit planes are written
+      if (lane == 0) {
+        const uint32_t plane16 = (uint32_t)L.plane >> 4;
+        bool ok = true;
+        for (int t = 0; t < nsub && ok; ++t) {
+          const int d = t % kGDStages;
+          ok = tc::mbar_wait(&bar_ready[d], (t / kGDStages) & 1, tc::kWaitPolls);
+          if (!ok) break;
+          tc::fence_after_sync();
+          const uint32_t sbase = tc::smem_addr(dbase + d * L.dstage);
+          const uint64_t adesc = tc::desc_kmajor(sbase, tc::kCoreBytes, kGSbo);
+          const uint64_t bdesc = tc::desc_kmajor(sbase + (uint32_t)L.bstack, tc::kCoreBytes, kGSbo);
+          GramStack<0>::issue(tmem, adesc, bdesc, plane16, t == 0);
+          tc::commit(&bar_dfree[d]);
+        }
+        if (ok && nsub > 0) {
+          const int tl = nsub - 1;
+          ok = tc::mbar_wait(&bar_dfree[tl % kGDStages], (tl / kGDStages) & 1, tc::kWaitPolls);
+        }
+        if (!ok) atomicExch(&s_err, 1);
+      }
+    } else {
+      // ---- slicing warps: every sub-tile, FP64 stage -> digit planes and the stacked B copy
+      const int ntask = (mp16 / 16) * 4;                  // warp tasks: 16 columns x 2 row octets
+      for (int t = 0; t < nsub; ++t) {
+        const int d = t % kGDStages, f = t % L.fstages;
+        bool ok = tc::mbar_wait(&bar_full[f], (t / L.fstages) & 1, tc::kWaitPolls);
+        if (ok && t >= kGDStages) ok = tc::mbar_wait(&bar_dfree[d], ((t / kGDStages) - 1) & 1, tc::kWaitPolls);
+        if (!ok || *reinterpret_cast<volatile int*>(&s_err)) {
+          atomicExch(&s_err, 1);
+          break;
+        }
+        uint8_t* stage = dbase + d * L.dstage;
+        const double* fs = reinterpret_cast<const double*>(fbase + f * L.fstage);
+        const int nr = imin(kGSub, r1 - (r0 + t * kGSub));
+        for (int g = warp; g < ntask; g += kGSliceWarps) {
+          // lane -> (column, K octet) so that every half-warp reads 16 distinct columns of a
+          // staged row (conflict-free 8-byte loads) and writes 16 distinct bank pairs of the
+          // digit planes (conflict-free 8-byte stores): lanes 8-15 take the upper 8 columns
+          // of the odd octet, lanes 16-23 the upper 8 of the even one.
+          const int jg = g % (mp16 / 16), kg = g / (mp16 / 16);
+          const int j = jg * 16 + (lane & 7) + 8 * (((lane >> 3) ^ (lane >> 4)) & 1);
+          const int k8 = kg * 2 + ((lane >> 3) & 1);      // K octet: 0..3 rows of A, 4..7 rows of D
+          const int rq = (k8 & 3) * 8;
+          const double* src = fs + (size_t)((k8 >> 2) * kGSub + rq) * m + j;
+          double x0[4], x1[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            x0[q] = (j < m && rq + q < nr) ? src[(size_t)q * m] : 0.0;
+            x1[q] = (j < m && rq + 4 + q < nr) ? src[(size_t)(q + 4) * m] : 0.0;
+          }
+          uint32_t w0[oz::kDigits], w1[oz::kDigits];
+          oz::slice4(x0, s_sc[j], w0);
+          oz::slice4(x1, s_sc[j], w1);
+          const int off = tc::core_offset(j, k8 * 8, kGKBytes);
+#pragma unroll
+          for (int i = 0; i < oz::kDigits; ++i)
+            *reinterpret_cast<uint2*>(stage + i * L.plane + off) = make_uint2(w0[i], w1[i]);
+          const int jj = j - h * kGN;
+          if (jj >= 0 && jj < kGN) {                      // the CTA's own columns: the stacked B copy
+#pragma unroll
+            for (int i = 0; i < oz::kDigits; ++i)
+              *reinterpret_cast<uint2*>(stage + L.bstack + tc::core_offset(i * kGN + jj, k8 * 8, kGKBytes)) =
+                  make_uint2(w0[i], w1[i]);
+          }
+        }
+        tc::fence_smem_to_async();
+        __syncwarp();
+        if (lane == 0) {
+          tc::mbar_arrive(&bar_ffree[f]);
+          tc::mbar_arrive(&bar_ready[d]);
+        }
+      }
+    }
+  }
+
+  // readout: warp w < 8 reads TMEM lanes 32 (w & 3) .. + 31 (output rows) of output w >> 2 (Cr, G)
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const bool ok = s_err == 0;
+  if (warp < 8) {
+    const int quarter = warp & 3, out = warp >> 2;
+    const int i = quarter * 32 + lane;
+    double* dst = partial + (((size_t)b * nchunks + c) * 2 + out) * (size_t)m * m;
+    const uint32_t tbase = tc::tmem_at(tmem, quarter * 32, out * oz::kDigits * kGN);
+    for (int jc = 0; jc < kGN; jc += 8) {
+      uint32_t r[oz::kDigits][8];
+      if (!bad && ok) {
+#pragma unroll
+        for (int l = 0; l < oz::kDigits; ++l) tc::tmem_ld8(tbase + l * kGN + jc, r[l]);
+#pragma unroll
+        for (int l = 0; l < oz::kDigits; ++l) tc::tmem_wait8(r[l]);
+      }
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        const int col = h * kGN + jc + jj;
+        if (i < m && col < m) {
+          double v = __longlong_as_double(0x7FF8000000000000ll);   // NaN: non-finite input or a stall
+          if (!bad && ok) {
+            uint32_t a[oz::kDigits];
+#pragma unroll
+            for (int l = 0; l < oz::kDigits; ++l) a[l] = r[l][jj];
+            v = oz::horner6(a) * s_inv[i] * s_inv[col];
+          }
+          dst[(size_t)i * m + col] = v;
+        }
+      }
+    }
+  }
+  if (!ok && !bad) {
+    if (tid == 0) atomicExch(stall, 1);
+    // drain: let committed MMAs and issued copies finish before TMEM and shared memory are released
+    if (tid == 0) {
+      for (int s = 0; s < kGDStages; ++s) (void)tc::mbar_wait(&bar_dfree[s], 0, tc::kWaitPolls);
+      for (int s = 0; s < L.fstages; ++s) (void)tc::mbar_wait(&bar_full[s], 0, tc::kWaitPolls);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tmem, kGTmemCols);
+}
+
+struct OzGramPlan {
+  int chunk, nchunks, ncg;
+};
+
+int sm_count_oz() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+// Row chunks per instance: the count minimising waves x chunk length (one CTA per
+// SM), chunks a multiple of the pre-pass block and short enough for exact INT32.
+OzGramPlan oz_gram_plan(int batch, int rows, int m) {
+  const int sms = sm_count_oz();
+  const int ncg = cdiv(m, kGN);
+  const int max_chunk = 8192;                     // K = 2 chunk rows: 6 x 2^14 x 2 x 8192 < 2^31
+  int best = 1;
+  double best_cost = 1e300;
+  for (int nc = 1; nc <= 32; ++nc) {
+    const int chunk = round_up(cdiv(rows, nc), kScaleRows);
+    if (chunk > max_chunk) continue;
+    const int used = cdiv(rows, chunk);
+    const long long ctas = (long long)batch * used * ncg;
+    const double cost = (double)((ctas + sms - 1) / sms) * chunk * (1.0 + 0.01 * used);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = nc;
+    }
+  }
+  const int chunk = round_up(cdiv(rows, best), kScaleRows);
+  return OzGramPlan{chunk, cdiv(rows, chunk), ncg};
+}
+
+size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+}  // namespace
+
+size_t ozaki_gram_workspace_bytes(int batch, int rows, int m) {
+  const OzGramPlan pl = oz_gram_plan(batch, rows, m);
+  return align256(sizeof(double) * (size_t)batch * pl.nchunks * 2 * m * m) +
+         align256(sizeof(unsigned long long) * (size_t)batch * pl.nchunks * m);
+}
+
+cudaError_t launch_gram_ozaki(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
+                              int batch, int rows, int m, void* workspace, int32_t* row_exp, int* stall,
+                              cudaStream_t stream) {
+  const OzGramPlan pl = oz_gram_plan(batch, rows, m);
+  double* partial = static_cast<double*>(workspace);
+  unsigned long long* col_bits = reinterpret_cast<unsigned long long*>(
+      static_cast<char*>(workspace) + align256(sizeof(double) * (size_t)batch * pl.nchunks * 2 * m * m));
+  cudaError_t err = cudaMemsetAsync(col_bits, 0, sizeof(unsigned long long) * (size_t)batch * pl.nchunks * m, stream);
+  if (err != cudaSuccess) return err;
+  ozaki_scale_kernel<<<dim3(cdiv(rows, kScaleRows), batch), kScaleThreads, 0, stream>>>(
+      A, D, ab_stride, rows, m, pl.chunk, pl.nchunks, col_bits, row_exp);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  const int smem = gram_smem(m).total;
+  err = cudaFuncSetAttribute(ozaki_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (err != cudaSuccess) return err;
+  ozaki_gram_kernel<<<dim3(pl.nchunks * pl.ncg, batch), kGThreads, smem, stream>>>(
+      A, D, ab_stride, rows, m, pl.chunk, pl.nchunks, pl.ncg, col_bits, partial, stall);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  return launch_gram_finalize(partial, Cr, Ci, batch, m, pl.nchunks, stream);
 }
 
 }  // namespace ssn

@@ -112,6 +112,25 @@ __device__ __forceinline__ void fence_smem_to_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Plain arrive (count 1) on the mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_addr(mbar)) : "memory");
+}
+
+// Arrive once on the mbarrier and add `bytes` to the transaction count its phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(mbar)), "r"(bytes)
+               : "memory");
+}
+
+// Bulk (non-tensor) asynchronous copy of `bytes` contiguous bytes from global to this CTA's
+// shared memory, completing as transactions on the mbarrier.  dst, src 16-byte aligned,
+// bytes a multiple of 16.  No multicast.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(mbar)) : "memory");
+}
+
 // TMEM address of (lane, column).
 __device__ __forceinline__ uint32_t tmem_at(uint32_t base, int lane, int col) {
   return base + (static_cast<uint32_t>(lane) << 16) + static_cast<uint32_t>(col);

@@ -27,7 +27,7 @@ PROTOTYPES = {
     "ssn_workspace_bytes": (_SZ, [_I, _I, _I]),
     "ssn_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_gram_workspace_bytes": (_SZ, [_I, _I, _I]),
-    "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P]),
+    "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_gram_noalloc_scratch_bytes": (_SZ, []),
     "ssn_gram_noalloc": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P]),
     "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P]),

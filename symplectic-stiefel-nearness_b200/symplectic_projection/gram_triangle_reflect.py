@@ -10,8 +10,12 @@ def initialize_kernels():
 
 
 @torch.no_grad()
-def gram(A, D):
-    """Return (Cr, Ci) = (A^T A + D^T D, A^T D - D^T A) for CUDA float64 [batch, rows, m]."""
+def gram(A, D, precision="fp64"):
+    """Return (Cr, Ci) = (A^T A + D^T D, A^T D - D^T A) for CUDA float64 [batch, rows, m].
+
+    precision="split" uses the INT8 Ozaki tensor-core products (about 1e-12
+    relative to max|T|^2 per entry); "fp64" the FP64 tensor-core products.
+    """
     dev = N.require_cuda_f64(A, D)
     batch, rows, m = A.shape
     if D.shape != A.shape:
@@ -22,8 +26,10 @@ def gram(A, D):
     lib = N.load()
     nbytes = lib.ssn_gram_workspace_bytes(batch, rows, m)
     ws = workspace(dev, nbytes)
+    opt = N.options(precision=precision)
     N.check(lib.ssn_gram(A.data_ptr(), D.data_ptr(), rows * m, Cr.data_ptr(), Ci.data_ptr(),
-                         batch, rows, m, ws.data_ptr(), nbytes, N.stream_handle(dev)), "ssn_gram")
+                         batch, rows, m, ws.data_ptr(), nbytes, N.ctypes.byref(opt), N.stream_handle(dev)),
+            "ssn_gram")
     return Cr, Ci
 
 

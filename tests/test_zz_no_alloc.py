@@ -29,7 +29,7 @@ def _gram_with_workspace(lib, N, A, D):
     nbytes = lib.ssn_gram_workspace_bytes(batch, rows, m)
     ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     N.check(lib.ssn_gram(A.data_ptr(), D.data_ptr(), rows * m, Cr.data_ptr(), Ci.data_ptr(),
-                         batch, rows, m, ws.data_ptr(), nbytes, N.stream_handle(A.device)), "ssn_gram")
+                         batch, rows, m, ws.data_ptr(), nbytes, None, N.stream_handle(A.device)), "ssn_gram")
     return Cr, Ci
 
 
