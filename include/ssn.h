@@ -142,10 +142,18 @@ int ssn_gram_noalloc(const double* A, const double* D, int64_t ab_stride, double
  * A, D, Ur, Ui are [batch, rows, m] with batch strides ab_stride / u_stride;
  * P, Q are [batch, m, m] contiguous.  Replaces recover_block
  * (recovery_fused.py:19-30; kernel recover_fused, recovery_fused.cu:2-41).
+ * opt NULL or SSN_PRECISION_FP64: FP64 tensor-core (DMMA) products, no
+ * workspace (workspace may be NULL).  SSN_PRECISION_SPLIT: INT8 Ozaki
+ * products on the tcgen05 tensor cores (six balanced digits of every row of
+ * [A D] and of [P Q], [-Q P], exact INT32 accumulation, FP64 recombination;
+ * each entry within about 2^-45 K of its largest row contributions); needs
+ * ssn_recover_workspace_bytes of workspace.
  */
+size_t ssn_recover_workspace_bytes(int batch, int rows, int m);
 int ssn_recover(const double* A, const double* D, int64_t ab_stride,
                 const double* P, const double* Q, double* Ur, double* Ui, int64_t u_stride,
-                int batch, int rows, int m, ssn_stream_t stream);
+                int batch, int rows, int m, void* workspace, size_t workspace_bytes,
+                const ssn_options* opt, ssn_stream_t stream);
 
 /*
  * Symmetric eigendecomposition of the scaled Gram matrix, Cr / s = V diag(w) V^T

@@ -24,7 +24,7 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Workspace layout of ssn_solve (byte offsets, 256-byte aligned sections).
 struct SolveLayout {
-  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, eig_ws, row_exp, stall, total;
+  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, eig_ws, rec, stall, total;
 };
 
 SolveLayout solve_layout(int batch, int n, int m) {
@@ -51,7 +51,8 @@ SolveLayout solve_layout(int batch, int n, int m) {
   L.work = take(work > partial ? work : partial);
   L.eig_status = take(sizeof(int32_t) * batch);
   L.eig_ws = take(eigh_workspace_bytes(batch, m));
-  L.row_exp = take(sizeof(int32_t) * (size_t)batch * n);     // split form: per-row scales of [A_r | D_r]
+  // split form: the recovery's digits of [A | D] (made early, alongside the Newton phase)
+  L.rec = take(ozaki_recover_workspace_bytes(batch, n, m));
   L.stall = take(sizeof(int32_t) * 4);                        // split form: tensor-core wait-limit flag
   L.total = off;
   return L;
@@ -81,6 +82,30 @@ DualLayout dual_layout(int batch, int m) {
 }
 
 constexpr int kDefaultEigSweeps = 3;
+
+// A side stream forked from the caller's stream with events (and joined back the
+// same way), so work that only depends on the inputs can overlap later kernels.
+// Stream-capture safe: the fork and join are event record / wait pairs.  The
+// stream and events are created per call and released once their work is done.
+struct SideStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t forked = nullptr, done = nullptr;
+  cudaError_t fork(cudaStream_t parent) {
+    cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&forked, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(forked, parent);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, forked, 0);
+    return e;
+  }
+  cudaError_t record() { return cudaEventRecord(done, stream); }
+  cudaError_t join(cudaStream_t parent) { return cudaStreamWaitEvent(parent, done, 0); }
+  ~SideStream() {
+    if (done) cudaEventDestroy(done);
+    if (forked) cudaEventDestroy(forked);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
 
 void fill_options(const ssn_options* opt, DualArgs& a) {
   ssn_options d;
@@ -174,11 +199,20 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
   const int64_t stride = 2LL * n * m;
   const double* A = T;
   const double* D = T + (size_t)n * m;
-  int32_t* row_exp = reinterpret_cast<int32_t*>(ws + L.row_exp);
   int* stall = reinterpret_cast<int*>(ws + L.stall);
-  cudaError_t e = split_form(opt) ? launch_gram_ozaki(A, D, stride, Cr, Ci, batch, n, m, work, row_exp, stall, stream)
-                                  : launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
+  const bool split = split_form(opt);
+  cudaError_t e = split ? launch_gram_ozaki(A, D, stride, Cr, Ci, batch, n, m, work, nullptr, stall, stream)
+                        : launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
+  // split form: the digits of [A | D] for the recovery do not depend on the dual solution, so
+  // they are made on a side stream while the (latency-bound) eigen and Newton kernels run
+  SideStream side;
+  if (split) {
+    e = side.fork(stream);
+    if (e == cudaSuccess) e = launch_recover_wdigits(A, D, stride, batch, n, m, ws + L.rec, side.stream);
+    if (e == cudaSuccess) e = side.record();
+    if (e != cudaSuccess) return SSN_ERR_CUDA;
+  }
   e = eigenbasis(opt, Cr, values, vectors, scale, nullptr, eig_status, batch, m, ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   DualArgs a{};
@@ -199,7 +233,13 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
   a.counters = nullptr;
   e = launch_dual(a, batch, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
-  e = launch_recover(A, D, stride, Pf, Qf, X, X + (size_t)n * m, stride, batch, n, m, stream);
+  if (split) {
+    e = side.join(stream);
+    if (e == cudaSuccess)
+      e = launch_recover_products(Pf, Qf, X, X + (size_t)n * m, stride, batch, n, m, ws + L.rec, stream);
+  } else {
+    e = launch_recover(A, D, stride, Pf, Qf, X, X + (size_t)n * m, stride, batch, n, m, stream);
+  }
   return cuda_status(e);
 }
 
@@ -229,15 +269,27 @@ int ssn_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, do
   return cuda_status(launch_gram(A, D, ab_stride, Cr, Ci, batch, rows, m, static_cast<double*>(workspace), st));
 }
 
+size_t ssn_recover_workspace_bytes(int batch, int rows, int m) {
+  if (!shape_ok(batch, m) || rows < 1) return 0;
+  return ozaki_recover_workspace_bytes(batch, rows, m);
+}
+
 int ssn_recover(const double* A, const double* D, int64_t ab_stride, const double* P, const double* Q,
-                double* Ur, double* Ui, int64_t u_stride, int batch, int rows, int m,
-                ssn_stream_t stream) {
+                double* Ur, double* Ui, int64_t u_stride, int batch, int rows, int m, void* workspace,
+                size_t workspace_bytes, const ssn_options* opt, ssn_stream_t stream) {
   if (!shape_ok(batch, m) || rows < 1 || !A || !D || !P || !Q || !Ur || !Ui ||
       ab_stride < (int64_t)rows * m || u_stride < (int64_t)rows * m || (ab_stride % 2) != 0 ||
-      (u_stride % 2) != 0 || !aligned16(A) || !aligned16(D) || !aligned16(P) || !aligned16(Q))
+      (u_stride % 2) != 0 || !aligned16(A) || !aligned16(D) || !aligned16(P) || !aligned16(Q) ||
+      !options_ok(opt))
     return SSN_ERR_INVALID_ARGUMENT;
-  return cuda_status(launch_recover(A, D, ab_stride, P, Q, Ur, Ui, u_stride, batch, rows, m,
-                                    reinterpret_cast<cudaStream_t>(stream)));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (split_form(opt)) {
+    if (!workspace || workspace_bytes < ozaki_recover_workspace_bytes(batch, rows, m) || !aligned16(workspace))
+      return SSN_ERR_WORKSPACE;
+    return cuda_status(launch_recover_ozaki(A, D, ab_stride, P, Q, Ur, Ui, u_stride, batch, rows, m,
+                                            workspace, st));
+  }
+  return cuda_status(launch_recover(A, D, ab_stride, P, Q, Ur, Ui, u_stride, batch, rows, m, st));
 }
 
 size_t ssn_eigh_workspace_bytes(int batch, int m) {

@@ -67,6 +67,17 @@ size_t ozaki_gram_workspace_bytes(int batch, int rows, int m);
 cudaError_t launch_gram_ozaki(const double* A, const double* D, int64_t ab_stride, double* Cr, double* Ci,
                               int batch, int rows, int m, void* workspace, int32_t* row_exp, int* stall,
                               cudaStream_t stream);
+// Split-precision (INT8 Ozaki, tcgen05) recovery Ur = A P^T + D Q^T, Ui = D P^T - A Q^T in two parts:
+// the digits of W = [A | D] (independent of P, Q, so they can run early on another stream),
+// then the products.  Both use the same workspace (ozaki_recover_workspace_bytes).
+size_t ozaki_recover_workspace_bytes(int batch, int rows, int m);
+cudaError_t launch_recover_wdigits(const double* A, const double* D, int64_t ab_stride, int batch, int rows, int m,
+                                   void* workspace, cudaStream_t stream);
+cudaError_t launch_recover_products(const double* P, const double* Q, double* Ur, double* Ui, int64_t u_stride,
+                                    int batch, int rows, int m, void* workspace, cudaStream_t stream);
+cudaError_t launch_recover_ozaki(const double* A, const double* D, int64_t ab_stride, const double* P,
+                                 const double* Q, double* Ur, double* Ui, int64_t u_stride, int batch, int rows,
+                                 int m, void* workspace, cudaStream_t stream);
 cudaError_t launch_recover(const double* A, const double* D, int64_t ab_stride, const double* P,
                            const double* Q, double* Ur, double* Ui, int64_t u_stride, int batch,
                            int rows, int m, cudaStream_t stream);

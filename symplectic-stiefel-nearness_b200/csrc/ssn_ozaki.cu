@@ -191,8 +191,9 @@ constexpr int kScaleThreads = 256;
 constexpr int kScaleRows = 64;                 // rows of A and D per pre-pass block
 
 // Pre-pass: per-(chunk, column) max |x| over the rows of A and D in the chunk (as
-// bit patterns, atomicMax into a zeroed array; max is order-independent) and
-// the per-row scale exponent of [A_r | D_r] for the recovery.
+// bit patterns, atomicMax into a zeroed array; max is order-independent; skipped
+// when col_bits is null) and the per-row scale exponent of [A_r | D_r] for the
+// recovery (skipped when row_exp is null).
 __global__ void __launch_bounds__(kScaleThreads)
     ozaki_scale_kernel(const double* __restrict__ A, const double* __restrict__ D, int64_t ab_stride, int rows,
                        int m, int chunk, int nchunks, unsigned long long* __restrict__ col_bits,
@@ -233,11 +234,12 @@ __global__ void __launch_bounds__(kScaleThreads)
   }
   __syncthreads();
   const int c = r0 / chunk;        // pre-pass blocks never straddle a chunk (chunk % kScaleRows == 0)
-  for (int j = threadIdx.x; j < m; j += kScaleThreads) {
-    unsigned long long mx = 0ull;
-    for (int w = 0; w < kScaleThreads / 32; ++w) mx = max(mx, cmax[w][j]);
-    atomicMax(&col_bits[((size_t)b * nchunks + c) * m + j], mx);
-  }
+  if (col_bits)
+    for (int j = threadIdx.x; j < m; j += kScaleThreads) {
+      unsigned long long mx = 0ull;
+      for (int w = 0; w < kScaleThreads / 32; ++w) mx = max(mx, cmax[w][j]);
+      atomicMax(&col_bits[((size_t)b * nchunks + c) * m + j], mx);
+    }
 }
 
 // Warp roles.  All slicing warps work on every sub-tile in order, so every
@@ -566,6 +568,398 @@ cudaError_t launch_gram_ozaki(const double* A, const double* D, int64_t ab_strid
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   return launch_gram_finalize(partial, Cr, Ci, batch, m, pl.nchunks, stream);
+}
+
+// ============================================================== Ozaki recovery
+//
+// X = [A P^T + D Q^T ; D P^T - A Q^T].  With W_r = [A_r | D_r] (K = 2m) every
+// entry is R[r, o] = sum_c W[r, c] B[o, c] for the 2m output columns o (Ur then
+// Ui) with B rows [P_o | Q_o] (o < m) and [-Q_o' | P_o'] (o' = o - m); per-row
+// scales on both sides (W rows from the Gram pre-pass, B rows from the prep
+// kernel), six digits each, so X is accurate to about 2^-46 of each row's
+// largest contribution.
+//
+// One CTA per (instance, group of 64 output columns, part of the row tiles),
+// persistent over its tiles: MMA M = a 128-row tile, N = stacked digits of the
+// group's 64 B rows, K = 2m in 32-byte steps.  The prep kernel slices B once per
+// (instance, group) into the stacked, step-major layout the CTA bulk-loads in
+// one copy; sixteen slicing warps load W straight from global memory two steps
+// ahead of the step they slice; the MMA warp runs a tile's steps once the
+// epilogue warps have drained the previous tile's accumulators (six levels of
+// 64 columns: 384 TMEM columns).
+namespace {
+
+constexpr int kRM = 128;                                  // rows per tile (MMA M)
+constexpr int kRW = 64;                                   // output columns per CTA
+constexpr int kRK = 32;                                   // K bytes per step
+constexpr int kRPlane = kRM * kRK;                        // 4096: one digit plane of a step
+constexpr int kRAStage = oz::kDigits * kRPlane;           // 24576: the six A planes of a step
+constexpr int kRBStep = oz::kDigits * kRW * kRK;          // 12288: stacked B digits of a step
+constexpr int kRStagesMax = 4;                            // digit-plane stages (bulk copies of W digits)
+constexpr int kRMmaWarp = 0;                              // warp 0: MMA issuer (lane 0), TMEM allocator
+constexpr int kRLoadWarp = 1;                             // warp 1: bulk copies of the W digit steps
+constexpr int kREpiWarp0 = 4;                             // warps 4-7: epilogue, TMEM lane quarter = warp % 4
+constexpr int kRThreads = 8 * 32;
+constexpr int kRSmemMax = 227 * 1024 - 1024;              // opt-in limit minus the static shared memory
+constexpr uint32_t kRSbo = (kRK / 16) * tc::kCoreBytes;    // 256
+constexpr uint32_t kRTmemCols = 512;                      // 6 x 64 = 384 used
+
+__host__ __device__ inline int rec_groups(int m) { return cdiv(2 * m, kRW); }
+__host__ __device__ inline int rec_steps(int m) { return cdiv(2 * m, kRK); }
+constexpr int kREpiLd = 9;                                // padded row stride (doubles) of the epilogue transpose
+constexpr int kREpiBuf = 32 * kREpiLd * 8;                // 2304 bytes per epilogue warp
+__host__ __device__ inline int rec_stages(int m) {
+  const int f = (kRSmemMax - rec_steps(m) * kRBStep - 4 * kREpiBuf) / kRAStage;
+  return f > kRStagesMax ? kRStagesMax : f;
+}
+__host__ __device__ inline int rec_smem(int m) {
+  return rec_steps(m) * kRBStep + rec_stages(m) * kRAStage + 4 * kREpiBuf;
+}
+
+// B row o, column c (o < 2m, c < 2m): rows [P_o | Q_o] (Ur), [-Q_o' | P_o'] (Ui).
+__device__ __forceinline__ double rec_b(const double* P, const double* Q, int m, int o, int c) {
+  if (o < m) return c < m ? P[o * m + c] : Q[o * m + c - m];
+  const int oo = o - m;
+  return c < m ? -Q[oo * m + c] : P[oo * m + c - m];
+}
+
+// One warp per B row: its scale exponent and its six digits, written in the
+// stacked step-major layout [instance][group][step][digit q][64 rows][32 K bytes]
+// (K-major core matrices), zero outside o < 2m, c < 2m.
+__global__ void __launch_bounds__(256)
+    ozaki_recover_prep_kernel(const double* __restrict__ P, const double* __restrict__ Q, int m,
+                              uint8_t* __restrict__ bdig, int32_t* __restrict__ fexp) {
+  // grid.x = group x 8: each CTA (8 warps) handles 8 of the group's 64 B rows
+  const int h = blockIdx.x >> 3, b = blockIdx.y, ngrp = gridDim.x >> 3, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nks = rec_steps(m), kpad = nks * kRK;
+  const double* Pb = P + (size_t)b * m * m;
+  const double* Qb = Q + (size_t)b * m * m;
+  uint8_t* out = bdig + ((size_t)b * ngrp + h) * nks * kRBStep;
+  {
+    const int jj = (blockIdx.x & 7) * 8 + warp;
+    const int o = h * kRW + jj;
+    unsigned long long mx = 0ull;
+    if (o < 2 * m)
+      for (int c = lane; c < 2 * m; c += 32) mx = max(mx, oz::abs_bits(rec_b(Pb, Qb, m, o, c)));
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
+    int e = oz::exp_of_maxbits(mx);
+    if (lane == 0 && o < 2 * m) fexp[(size_t)b * 2 * m + o] = e;
+    if (e == oz::kExpNonFinite) e = 0;
+    const double sc = oz::pow2(oz::kFrac - e);
+    for (int c = lane; c < kpad; c += 32) {
+      const double x = (o < 2 * m && c < 2 * m) ? rec_b(Pb, Qb, m, o, c) : 0.0;
+      const double z = fma(x, sc, oz::kMagic);
+      const uint32_t lo = static_cast<uint32_t>(__double2loint(z)), hi = static_cast<uint32_t>(__double2hiint(z));
+      const int s = c / kRK, k = c - s * kRK;
+#pragma unroll
+      for (int q = 0; q < oz::kDigits; ++q) {
+        const int byte = oz::kDigits - 1 - q;           // digit q is byte 5 - q of F + C
+        const uint32_t word = byte < 4 ? lo : hi;
+        const uint8_t d = static_cast<uint8_t>(((word >> (8 * (byte & 3))) & 0xFFu) ^ 0x80u);
+        out[(size_t)s * kRBStep + tc::core_offset(q * kRW + jj, k, kRK)] = d;
+      }
+    }
+  }
+}
+
+// The MMAs of one K step: for digit p of the tile rows, B = stacked digits
+// q0 .. q0 + NQ - 1 of the group's 64 rows, accumulated at TMEM columns 64 (p + q0).
+template <int P, int Q0, int NQ>
+__device__ __forceinline__ void rec_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, bool first) {
+  constexpr uint32_t idesc = tc::idesc_s8(kRM, NQ * kRW);
+  const uint64_t da = adesc + (uint64_t)((P * kRPlane) >> 4);
+  const uint64_t db = bdesc + (uint64_t)((Q0 * (kRW / 8) * kRSbo) >> 4);
+  tc::mma_s8(tmem + (uint32_t)(P + Q0) * kRW, da, db, idesc, (first && P == 0) ? 0u : 1u);
+}
+
+__device__ __forceinline__ void rec_step_mmas(uint32_t tmem, uint64_t adesc, uint64_t bdesc, bool first) {
+  rec_mma<0, 0, 4>(tmem, adesc, bdesc, first);
+  rec_mma<0, 4, 2>(tmem, adesc, bdesc, first);
+  rec_mma<1, 0, 4>(tmem, adesc, bdesc, first);
+  rec_mma<1, 4, 1>(tmem, adesc, bdesc, first);
+  rec_mma<2, 0, 4>(tmem, adesc, bdesc, first);
+  rec_mma<3, 0, 3>(tmem, adesc, bdesc, first);
+  rec_mma<4, 0, 2>(tmem, adesc, bdesc, first);
+  rec_mma<5, 0, 1>(tmem, adesc, bdesc, first);
+}
+
+// W digits: one warp per row of W = [A_r | D_r]: its scale exponent (max over
+// the row) and its six digits, written straight into the MMA layout of the
+// recovery: [instance][tile][step][digit q][128 rows][32 K bytes] (K-major core
+// matrices, zero beyond c < 2m and r < rows), so each (tile, step) is one
+// contiguous 24 KB block.  Lane l handles K octet l (columns 8 l .. 8 l + 7).
+__global__ void __launch_bounds__(256)
+    ozaki_wdigits_kernel(const double* __restrict__ A, const double* __restrict__ D, int64_t ab_stride, int rows,
+                         int m, uint8_t* __restrict__ wdig, int32_t* __restrict__ row_exp) {
+  const int tile = blockIdx.x, b = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nks = rec_steps(m), ntiles = gridDim.x;
+  const double* Ab = A + (size_t)b * ab_stride;
+  const double* Db = D + (size_t)b * ab_stride;
+  uint8_t* out = wdig + ((size_t)b * ntiles + tile) * nks * kRAStage;
+  const int c0 = lane * 8;                             // this lane's K octet
+  const bool active = c0 < nks * kRK;                 // octets of the padded K range
+  for (int rr = warp; rr < kRM; rr += 8) {
+    const int r = tile * kRM + rr;
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = c0 + 2 * i;                       // m even: a pair never straddles A and D
+      double2 v = make_double2(0.0, 0.0);
+      if (r < rows && c < 2 * m)
+        v = c < m ? __ldg(reinterpret_cast<const double2*>(Ab + (size_t)r * m + c))
+                  : __ldg(reinterpret_cast<const double2*>(Db + (size_t)r * m + (c - m)));
+      x[2 * i] = v.x;
+      x[2 * i + 1] = v.y;
+    }
+    unsigned long long mx = 0ull;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) mx = max(mx, oz::abs_bits(x[i]));
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
+    int e = oz::exp_of_maxbits(mx);
+    if (lane == 0 && r < rows) row_exp[(size_t)b * rows + r] = e;
+    if (e == oz::kExpNonFinite) e = 0;
+    if (!active) continue;
+    const double sc = oz::pow2(oz::kFrac - e);
+    const double x0[4] = {x[0], x[1], x[2], x[3]};
+    const double x1[4] = {x[4], x[5], x[6], x[7]};
+    uint32_t w0[oz::kDigits], w1[oz::kDigits];
+    oz::slice4(x0, sc, w0);
+    oz::slice4(x1, sc, w1);
+    const int s = c0 / kRK, k = c0 - s * kRK;
+    uint8_t* blk = out + (size_t)s * kRAStage + tc::core_offset(rr, k, kRK);
+#pragma unroll
+    for (int q = 0; q < oz::kDigits; ++q) *reinterpret_cast<uint2*>(blk + q * kRPlane) = make_uint2(w0[q], w1[q]);
+  }
+}
+
+// Persistent over the row tiles [tile0, tile1) of one (instance, output group):
+// the group's B digits are loaded once; warp 1 streams the W digit blocks of
+// every (tile, step) into a ring of stages; the MMA thread runs a tile's steps
+// once the epilogue has drained the previous tile's accumulators; the epilogue
+// warps recombine the levels and store X through a small shared transpose
+// (64-byte row segments).
+__global__ void __launch_bounds__(kRThreads, 1)
+    ozaki_recover_kernel(const uint8_t* __restrict__ wdig, const int32_t* __restrict__ row_exp,
+                         const uint8_t* __restrict__ bdig, const int32_t* __restrict__ fexp, double* __restrict__ Ur,
+                         double* __restrict__ Ui, int64_t u_stride, int rows, int m, int nparts,
+                         int* __restrict__ stall) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ uint64_t bar_b;
+  __shared__ uint64_t bar_full[kRStagesMax];     // a W digit step landed
+  __shared__ uint64_t bar_dfree[kRStagesMax];    // MMAs done with a stage
+  __shared__ uint64_t bar_acc_full;              // MMA commit: a tile's accumulators are complete
+  __shared__ uint64_t bar_acc_free;              // epilogue: a tile's accumulators have been read
+  __shared__ uint32_t tmem_slot;
+  __shared__ int s_err;
+  __shared__ double s_finv[kRW];                 // 2^(f_o - 26); NaN marks a non-finite B row
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ngrp = rec_groups(m), nks = rec_steps(m), ntiles = cdiv(rows, kRM), nst = rec_stages(m);
+  const int part = blockIdx.x % nparts, h = (blockIdx.x / nparts) % ngrp, b = blockIdx.y;
+  const int per = cdiv(ntiles, nparts);
+  const int tile0 = part * per, tile1 = imin(ntiles, tile0 + per);
+  const int ntl = imax(0, tile1 - tile0);
+  const int32_t* rexp = row_exp + (size_t)b * rows;
+  uint8_t* bsm = smem;                                              // nks x kRBStep
+  uint8_t* asm_ = smem + nks * kRBStep;                             // nst x kRAStage
+  double* ebuf = reinterpret_cast<double*>(asm_ + nst * kRAStage);  // 4 x kREpiBuf bytes
+  const double nan = __longlong_as_double(0x7FF8000000000000ll);
+
+  if (tid < kRW) {
+    const int o = h * kRW + tid;
+    const int e = o < 2 * m ? fexp[(size_t)b * 2 * m + o] : oz::kExpMin;
+    s_finv[tid] = e == oz::kExpNonFinite ? nan : oz::pow2(e - 26);
+  }
+  if (tid == 0) {
+    tc::mbar_init(&bar_b, 1);
+    for (int s = 0; s < kRStagesMax; ++s) {
+      tc::mbar_init(&bar_full[s], 1);
+      tc::mbar_init(&bar_dfree[s], 1);
+    }
+    tc::mbar_init(&bar_acc_full, 1);
+    tc::mbar_init(&bar_acc_free, 4);
+    s_err = 0;
+  }
+  if (warp == kRMmaWarp) tc::tmem_alloc(&tmem_slot, kRTmemCols);
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const int nsteps = ntl * nks;
+
+  if (warp == kRMmaWarp) {
+    // ---- MMA thread: the group's B digits once, then per tile 8 MMAs per K step
+    if (lane == 0 && ntl > 0) {
+      const uint32_t bbytes = (uint32_t)(nks * kRBStep);
+      tc::mbar_arrive_expect_tx(&bar_b, bbytes);
+      tc::bulk_g2s(bsm, bdig + ((size_t)b * ngrp + h) * bbytes, bbytes, &bar_b);
+      bool ok = tc::mbar_wait(&bar_b, 0, tc::kWaitPolls);
+      int g = 0;                                                      // K step counter over all tiles
+      for (int it = 0; it < ntl && ok; ++it) {
+        if (it > 0) ok = tc::mbar_wait(&bar_acc_free, (it - 1) & 1, tc::kWaitPolls);
+        tc::fence_after_sync();
+        for (int s = 0; s < nks && ok; ++s, ++g) {
+          const int d = g % nst;
+          ok = tc::mbar_wait(&bar_full[d], (g / nst) & 1, tc::kWaitPolls);
+          if (!ok) break;
+          const uint64_t adesc = tc::desc_kmajor(tc::smem_addr(asm_ + d * kRAStage), tc::kCoreBytes, kRSbo);
+          const uint64_t bdesc = tc::desc_kmajor(tc::smem_addr(bsm + s * kRBStep), tc::kCoreBytes, kRSbo);
+          rec_step_mmas(tmem, adesc, bdesc, s == 0);
+          tc::commit(&bar_dfree[d]);
+        }
+        if (ok) tc::commit(&bar_acc_full);
+      }
+      if (!ok) atomicExch(&s_err, 1);
+    }
+  } else if (warp == kRLoadWarp) {
+    // ---- W digit steps: one 24 KB bulk copy per (tile, step) into the stage ring
+    if (lane == 0) {
+      for (int g = 0; g < nsteps; ++g) {
+        const int d = g % nst;
+        if (g >= nst && !tc::mbar_wait(&bar_dfree[d], ((g / nst) - 1) & 1, tc::kWaitPolls)) {
+          atomicExch(&s_err, 1);
+          break;
+        }
+        if (*reinterpret_cast<volatile int*>(&s_err)) break;
+        const int it = g / nks, s = g - it * nks;
+        const uint8_t* src = wdig + (((size_t)b * ntiles + tile0 + it) * nks + s) * kRAStage;
+        tc::mbar_arrive_expect_tx(&bar_full[d], kRAStage);
+        tc::bulk_g2s(asm_ + d * kRAStage, src, kRAStage, &bar_full[d]);
+      }
+    }
+  } else if (warp >= kREpiWarp0) {
+    // ---- epilogue warps: TMEM lane quarter (warp % 4); 64 output columns of 32 rows
+    const int ew = warp - kREpiWarp0, quarter = warp & 3;
+    double* buf = ebuf + ew * (kREpiBuf / 8);
+    const uint32_t tbase = tc::tmem_at(tmem, quarter * 32, 0);
+    for (int it = 0; it < ntl; ++it) {
+      bool ok = tc::mbar_wait(&bar_acc_full, it & 1, tc::kWaitPolls) && !*reinterpret_cast<volatile int*>(&s_err);
+      tc::fence_after_sync();
+      const int r0 = (tile0 + it) * kRM;
+      const int rr = quarter * 32 + lane, r = r0 + rr;
+      const int e = r < rows ? __ldg(rexp + r) : oz::kExpMin;
+      const double rinv = e == oz::kExpNonFinite ? nan : oz::pow2(e - 26);
+      for (int jc = 0; jc < kRW; jc += 8) {
+        uint32_t v[oz::kDigits][8];
+        if (ok) {
+#pragma unroll
+          for (int l = 0; l < oz::kDigits; ++l) tc::tmem_ld8(tbase + l * kRW + jc, v[l]);
+#pragma unroll
+          for (int l = 0; l < oz::kDigits; ++l) tc::tmem_wait8(v[l]);
+        }
+        if (jc + 8 == kRW) {                         // all of this tile's TMEM reads are done
+          tc::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive(&bar_acc_free);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          double corr = nan;
+          if (ok) {
+            uint32_t a[oz::kDigits];
+#pragma unroll
+            for (int l = 0; l < oz::kDigits; ++l) a[l] = v[l][jj];
+            corr = oz::horner6(a) * rinv * s_finv[jc + jj];
+          }
+          buf[lane * kREpiLd + jj] = corr;
+        }
+        __syncwarp();
+        // transposed write-out: 4 rows x 8 columns (64-byte row segments) per instruction
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int lr = k * 4 + (lane >> 3), cc = lane & 7;
+          const int rw = r0 + quarter * 32 + lr, o = h * kRW + jc + cc;
+          if (rw < rows && o < 2 * m) {
+            const double cv = buf[lr * kREpiLd + cc];
+            if (o < m) Ur[(size_t)b * u_stride + (size_t)rw * m + o] = cv;
+            else Ui[(size_t)b * u_stride + (size_t)rw * m + (o - m)] = cv;
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (s_err && tid == 0) {
+    atomicExch(stall, 1);
+    // drain: let committed MMAs and issued copies finish before TMEM and shared memory are released
+    for (int s = 0; s < nst; ++s) (void)tc::mbar_wait(&bar_dfree[s], 0, tc::kWaitPolls);
+    for (int s = 0; s < nst; ++s) (void)tc::mbar_wait(&bar_full[s], 0, tc::kWaitPolls);
+    (void)tc::mbar_wait(&bar_b, 0, tc::kWaitPolls);
+  }
+  __syncthreads();
+  if (warp == kRMmaWarp) tc::tmem_dealloc(tmem, kRTmemCols);
+}
+
+}  // namespace
+
+size_t ozaki_recover_workspace_bytes(int batch, int rows, int m) {
+  return align256(sizeof(int32_t) * (size_t)batch * rows) +
+         align256((size_t)batch * cdiv(rows, kRM) * rec_steps(m) * kRAStage) +
+         align256((size_t)batch * rec_groups(m) * rec_steps(m) * kRBStep) +
+         align256(sizeof(int32_t) * (size_t)batch * 2 * m) + 256;
+}
+
+namespace {
+struct RecWs {
+  int32_t* row_exp;
+  uint8_t* wdig;
+  uint8_t* bdig;
+  int32_t* fexp;
+  int* stall;
+};
+RecWs rec_ws(void* workspace, int batch, int rows, int m) {
+  char* ws = static_cast<char*>(workspace);
+  RecWs w;
+  w.row_exp = reinterpret_cast<int32_t*>(ws);
+  ws += align256(sizeof(int32_t) * (size_t)batch * rows);
+  w.wdig = reinterpret_cast<uint8_t*>(ws);
+  ws += align256((size_t)batch * cdiv(rows, kRM) * rec_steps(m) * kRAStage);
+  w.bdig = reinterpret_cast<uint8_t*>(ws);
+  ws += align256((size_t)batch * rec_groups(m) * rec_steps(m) * kRBStep);
+  w.fexp = reinterpret_cast<int32_t*>(ws);
+  ws += align256(sizeof(int32_t) * (size_t)batch * 2 * m);
+  w.stall = reinterpret_cast<int*>(ws);
+  return w;
+}
+}  // namespace
+
+cudaError_t launch_recover_wdigits(const double* A, const double* D, int64_t ab_stride, int batch, int rows, int m,
+                                   void* workspace, cudaStream_t stream) {
+  const RecWs w = rec_ws(workspace, batch, rows, m);
+  ozaki_wdigits_kernel<<<dim3(cdiv(rows, kRM), batch), 256, 0, stream>>>(A, D, ab_stride, rows, m, w.wdig,
+                                                                          w.row_exp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_recover_products(const double* P, const double* Q, double* Ur, double* Ui, int64_t u_stride,
+                                    int batch, int rows, int m, void* workspace, cudaStream_t stream) {
+  const RecWs w = rec_ws(workspace, batch, rows, m);
+  ozaki_recover_prep_kernel<<<dim3(rec_groups(m) * 8, batch), 256, 0, stream>>>(P, Q, m, w.bdig, w.fexp);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  const int smem = rec_smem(m);
+  err = cudaFuncSetAttribute(ozaki_recover_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (err != cudaSuccess) return err;
+  // tiles of an (instance, group) split into parts: about four CTAs per SM over the grid
+  const int ntiles = cdiv(rows, kRM), pairs = batch * rec_groups(m);
+  const int nparts = imax(1, imin(ntiles, cdiv(4 * sm_count_oz(), pairs)));
+  ozaki_recover_kernel<<<dim3(nparts * rec_groups(m), batch), kRThreads, smem, stream>>>(
+      w.wdig, w.row_exp, w.bdig, w.fexp, Ur, Ui, u_stride, rows, m, nparts, w.stall);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_recover_ozaki(const double* A, const double* D, int64_t ab_stride, const double* P,
+                                 const double* Q, double* Ur, double* Ui, int64_t u_stride, int batch, int rows,
+                                 int m, void* workspace, cudaStream_t stream) {
+  cudaError_t err = launch_recover_wdigits(A, D, ab_stride, batch, rows, m, workspace, stream);
+  if (err != cudaSuccess) return err;
+  return launch_recover_products(P, Q, Ur, Ui, u_stride, batch, rows, m, workspace, stream);
 }
 
 }  // namespace ssn

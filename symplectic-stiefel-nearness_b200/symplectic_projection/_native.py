@@ -30,7 +30,8 @@ PROTOTYPES = {
     "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_gram_noalloc_scratch_bytes": (_SZ, []),
     "ssn_gram_noalloc": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P]),
-    "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P]),
+    "ssn_recover_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_eigh_workspace_bytes": (_SZ, [_I, _I]),
     "ssn_eigh": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
     "ssn_dual_workspace_bytes": (_SZ, [_I, _I]),

@@ -2,6 +2,7 @@
 import torch
 
 from . import _native as N
+from ._workspace import workspace
 
 
 def initialize_kernels():
@@ -9,15 +10,23 @@ def initialize_kernels():
 
 
 @torch.no_grad()
-def recover_block(A, D, P, Q):
-    """Ur = A P^T + D Q^T, Ui = D P^T - A Q^T; A, D [batch, rows, m], P, Q [batch, m, m]."""
+def recover_block(A, D, P, Q, precision="fp64"):
+    """Ur = A P^T + D Q^T, Ui = D P^T - A Q^T; A, D [batch, rows, m], P, Q [batch, m, m].
+
+    precision="split": INT8 Ozaki tensor-core products (six balanced digits per
+    row, exact INT32 accumulation); "fp64": FP64 tensor-core products.
+    """
     dev = N.require_cuda_f64(A, D, P, Q)
     batch, rows, m = A.shape
     if D.shape != A.shape or P.shape != (batch, m, m) or Q.shape != (batch, m, m):
         raise ValueError("shape mismatch")
     A, D, P, Q = (x.contiguous() for x in (A, D, P, Q))
     Ur, Ui = torch.empty_like(A), torch.empty_like(A)
-    N.check(N.load().ssn_recover(A.data_ptr(), D.data_ptr(), rows * m, P.data_ptr(), Q.data_ptr(),
-                                 Ur.data_ptr(), Ui.data_ptr(), rows * m, batch, rows, m,
-                                 N.stream_handle(dev)), "ssn_recover")
+    lib = N.load()
+    nbytes = lib.ssn_recover_workspace_bytes(batch, rows, m)
+    ws = workspace(dev, nbytes)
+    opt = N.options(precision=precision)
+    N.check(lib.ssn_recover(A.data_ptr(), D.data_ptr(), rows * m, P.data_ptr(), Q.data_ptr(),
+                            Ur.data_ptr(), Ui.data_ptr(), rows * m, batch, rows, m, ws.data_ptr(), nbytes,
+                            N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_recover")
     return Ur, Ui

@@ -92,3 +92,65 @@ def test_ozaki_gram_zero_and_tiny_columns():
     assert torch.equal(Cr[:, 0], torch.zeros_like(Cr[:, 0]))
     scale = Cr64.abs().amax()
     assert float((Cr - Cr64).abs().max() / scale) < 1e-12
+
+
+# ---------------------------------------------------------------- recovery
+def _recover_split(T, P, Q):
+    from symplectic_projection.recovery_fused import recover_block
+    n = T.shape[1] // 2
+    Td = T.cuda()
+    Ur, Ui = recover_block(Td[:, :n], Td[:, n:], P.cuda(), Q.cuda(), precision="split")
+    torch.cuda.synchronize()
+    return Ur.cpu(), Ui.cpu()
+
+
+def _pq(batch, m, scale, seed):
+    """P, Q of a skew omega of the given size: P + iQ = (I + i omega)^-1."""
+    g = torch.Generator().manual_seed(seed)
+    W = torch.randn(batch, m, m, generator=g, dtype=torch.float64) * scale
+    W = (W - W.mT) / 2
+    P = torch.linalg.inv(torch.eye(m, dtype=torch.float64) + W @ W)
+    return P, -W @ P
+
+
+@pytest.mark.parametrize("n,k,batch,scale", [(77, 4, 2, 0.1), (512, 12, 3, 0.02), (4096, 48, 2, 0.02),
+                                             (333, 64, 2, 0.5), (100, 1, 3, 1.0), (1000, 20, 2, 3.0)])
+def test_ozaki_recover_error_bound(n, k, batch, scale):
+    T, _ = O.make_inputs(n, k, 2, batch)
+    m = 2 * k
+    P, Q = _pq(batch, m, scale, n + k)
+    Ur, Ui = _recover_split(T, P, Q)
+    Ur64, Ui64 = O.recover(T[:, :n], T[:, n:], P, Q)
+    # rows [P | Q] (Ur) and [-Q | P] (Ui): per-entry bound from the row maxima of both factors
+    W = torch.cat((T[:, :n], T[:, n:]), dim=2)                       # [batch, n, 2m]
+    B1 = torch.cat((P, Q), dim=2)
+    B2 = torch.cat((-Q, P), dim=2)
+    wmax = W.abs().amax(dim=2)                                       # [batch, n]
+    bound1 = 2 * (2 * m) * 2.0 ** -45 * wmax[:, :, None] * B1.abs().amax(dim=2)[:, None, :] + 1e-300
+    bound2 = 2 * (2 * m) * 2.0 ** -45 * wmax[:, :, None] * B2.abs().amax(dim=2)[:, None, :] + 1e-300
+    ulp = 2.0 ** -52 * (Ur64.abs() + 1e-300)
+    assert bool(((Ur - Ur64).abs() <= bound1 + 4 * ulp).all())
+    assert bool(((Ui - Ui64).abs() <= bound2 + 4 * 2.0 ** -52 * Ui64.abs()).all())
+
+
+def test_ozaki_recover_identity_within_digit_rounding():
+    # P = I, Q = 0: X = T up to the rounding of each row to 46 fraction bits of its largest entry
+    T, _ = O.make_inputs(300, 8, 3, 2)
+    m = 16
+    P = torch.eye(m, dtype=torch.float64).expand(2, m, m).contiguous()
+    Q = torch.zeros(2, m, m, dtype=torch.float64)
+    Ur, Ui = _recover_split(T, P, Q)
+    W = torch.cat((T[:, :300], T[:, 300:]), dim=2)
+    tol = 2.0 ** -46 * W.abs().amax(dim=2, keepdim=True)
+    assert bool(((Ur - T[:, :300]).abs() <= tol).all()) and bool(((Ui - T[:, 300:]).abs() <= tol).all())
+
+
+def test_ozaki_recover_nonfinite_row_is_flagged():
+    T, _ = O.make_inputs(200, 6, 4, 2)
+    T[1, 17, 3] = float("nan")
+    P, Q = _pq(2, 12, 0.1, 5)
+    Ur, Ui = _recover_split(T, P, Q)
+    assert not bool(torch.isfinite(Ur[1, 17]).all())
+    assert bool(torch.isfinite(Ur[0]).all()) and bool(torch.isfinite(Ui[0]).all())
+    Ur64, _ = O.recover(T[:1, :200], T[:1, 200:], P[:1], Q[:1])
+    assert float((Ur[0] - Ur64[0]).abs().max()) < 1e-12
