@@ -74,8 +74,24 @@ typedef struct {
   double feas_tol;   /* 1e-8: an instance is done when residual < feas_tol / 2 */
   int precision;     /* SSN_PRECISION_FP64 (default) or SSN_PRECISION_SPLIT */
   int eig_sweeps;    /* split form: Jacobi sweeps of the rough eigenbasis (0 = default 3, max 24) */
-  int reserved[6];
+  int preconditioner; /* SSN_PRECOND_* (0 = automatic) */
+  int reserved[5];
 } ssn_options;
+
+/* CG preconditioner (ssn_options.preconditioner). */
+enum {
+  /* the reference's for the FP64 form, the adaptive one for the split form */
+  SSN_PRECOND_AUTO = 0,
+  /* skew(R / (lambda_i + lambda_j)) in the eigenbasis of the scaled Gram: the
+   * reference's (dual_recommended_hvp.py:113-114), exact at omega = 0 */
+  SSN_PRECOND_EIGENBASIS = 1,
+  /* the diagonal of the Hessian at the current omega in the working basis,
+   * P_ii Sr_jj + P_jj Sr_ii - 2 P_ij Sr_ij + 2 Q_ij Si_ij (lambda_i + lambda_j at
+   * omega = 0), with the full rotated Gram in the sandwich.  No counterpart in
+   * the reference: it keeps CG short on ill-conditioned targets, where the
+   * reference's preconditioner lets CG saturate and the Newton cap is reached. */
+  SSN_PRECOND_ADAPTIVE = 2
+};
 
 /* Library version as 10000*major + 100*minor + patch. */
 int ssn_version(void);
@@ -187,8 +203,9 @@ int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, doubl
  * ssn_eigh (values, vectors, scale, and its per-instance status eig_status,
  * which may be NULL).  counters (may be NULL) receives int32 [batch, 4]:
  * Newton steps run, Hessian-vector products, line-search trials, fallbacks.
- * Cr (the unscaled Gram) is read only by the split form (opt->precision ==
- * SSN_PRECISION_SPLIT, where it is required) and may be NULL otherwise.
+ * Cr (the unscaled Gram) is read only with the full rotated Gram (the split
+ * form, or the adaptive preconditioner), where it is required; it may be NULL
+ * otherwise.
  * Replaces dual_batch (dual_recommended_hvp.py:109-191) after the eigh call.
  * Needs ssn_newton_workspace_bytes.
  */

@@ -152,16 +152,31 @@ class DualStats:
     cg_per_step: list = field(default_factory=list)
 
 
+def adaptive_denominator(P, Q, Sr, Si):
+    """Diagonal of the Hessian H(E) = Z - Z^T, Z = P E Sr - Q E Si, on the skew basis
+    e_i e_j^T - e_j e_i^T:  P_ii Sr_jj + P_jj Sr_ii - 2 P_ij Sr_ij + 2 Q_ij Si_ij.
+
+    NOT part of the reference: the restatement of this build's adaptive
+    preconditioner (preconditioner="adaptive").  At omega = 0 (P = I, Q = 0,
+    Sr = diag(lambda)) it equals the reference's lambda_i + lambda_j.
+    """
+    dP, dS = P.diagonal(dim1=-2, dim2=-1), Sr.diagonal(dim1=-2, dim2=-1)
+    return dP[..., :, None] * dS[..., None, :] + dP[..., None, :] * dS[..., :, None] - 2 * P * Sr + 2 * Q * Si
+
+
 @torch.no_grad()
 def dual_batch(Cr: torch.Tensor, Ci: torch.Tensor, stats: DualStats | None = None,
                max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
-               max_backtrack: int = MAX_BACKTRACK):
+               max_backtrack: int = MAX_BACKTRACK, preconditioner: str = "eigenbasis"):
     """Dual Newton–CG in the eigenbasis of the scaled Cr.
 
     Returns (omega, L, P, Q, iterations) in the original basis, where
     P + iQ = (I + i omega)^-1 is the inverse cached at the accepted step and
     L = chol(I + omega omega).  Raises RuntimeError on the Newton or
     line-search cap, like dual_recommended_hvp.py:189-191.
+    preconditioner="eigenbasis" is the reference's; "adaptive" is this build's
+    extension (``adaptive_denominator``, entries that are not positive fall back
+    to lambda_i + lambda_j), used for the CG steps.
     """
     batch, m, _ = Cr.shape
     eye = torch.eye(m, dtype=Cr.dtype).expand(batch, m, m)
@@ -208,9 +223,13 @@ def dual_batch(Cr: torch.Tensor, Ci: torch.Tensor, stats: DualStats | None = Non
             if stats is not None:
                 stats.cg_per_step.append(0)
         else:                                                    # :142-161
+            den_s = den
+            if preconditioner == "adaptive":
+                den_a = adaptive_denominator(P, Q, Sr, Si)
+                den_s = torch.where(den_a > 0, den_a, den)
             direction = torch.zeros_like(g)
             r = masked_neg_g
-            z = precondition(r, den)
+            z = precondition(r, den_s)
             first_z = z
             p = z.clone()
             rz = frob_inner(r, z)
@@ -229,7 +248,7 @@ def dual_batch(Cr: torch.Tensor, Ci: torch.Tensor, stats: DualStats | None = Non
                 cg_on &= frob_norm(r) > tol
                 if not bool(cg_on.any()):
                     break
-                z = precondition(r, den)
+                z = precondition(r, den_s)
                 rz_next = frob_inner(r, z)
                 beta = rz_next / torch.where(cg_on, rz, torch.ones_like(rz))
                 p = torch.where(cg_on[:, None, None], z + beta[:, None, None] * p, torch.zeros_like(p))

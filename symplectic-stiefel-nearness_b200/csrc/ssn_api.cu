@@ -115,8 +115,10 @@ void fill_options(const ssn_options* opt, DualArgs& a) {
   a.max_cg = opt->max_cg;
   a.max_backtrack = opt->max_backtrack;
   a.feas_tol = opt->feas_tol;
-  a.approx_basis = opt->precision == SSN_PRECISION_SPLIT ? 1 : 0;
-  a.orthogonalize = a.approx_basis;
+  const bool split = opt->precision == SSN_PRECISION_SPLIT;
+  a.adaptive_precond = opt->preconditioner == SSN_PRECOND_ADAPTIVE || (opt->preconditioner == SSN_PRECOND_AUTO && split);
+  a.approx_basis = (split || a.adaptive_precond) ? 1 : 0;    // full rotated Gram
+  a.orthogonalize = split ? 1 : 0;                            // FP32 rotations: refine V in FP64
 }
 
 bool split_form(const ssn_options* opt) { return opt && opt->precision == SSN_PRECISION_SPLIT; }
@@ -128,7 +130,8 @@ bool options_ok(const ssn_options* opt) {
          opt->max_cg <= 100000 && opt->max_backtrack >= 1 && opt->max_backtrack <= 1074 &&
          opt->feas_tol > 0.0 &&
          (opt->precision == SSN_PRECISION_FP64 || opt->precision == SSN_PRECISION_SPLIT) &&
-         opt->eig_sweeps >= 0 && opt->eig_sweeps <= 24;
+         opt->eig_sweeps >= 0 && opt->eig_sweeps <= 24 &&
+         opt->preconditioner >= SSN_PRECOND_AUTO && opt->preconditioner <= SSN_PRECOND_ADAPTIVE;
 }
 
 // Eigenbasis of the scaled Gram for either precision form.
@@ -360,7 +363,10 @@ int ssn_newton(const double* Cr, const double* Ci, const double* values, const d
   if (!shape_ok(batch, m) || !Ci || !values || !vectors || !scale || !omega || !P || !Q ||
       !iterations || !status || !options_ok(opt) || !aligned16(Ci) || !aligned16(vectors))
     return SSN_ERR_INVALID_ARGUMENT;
-  if (split_form(opt) && (!Cr || !aligned16(Cr))) return SSN_ERR_INVALID_ARGUMENT;
+  DualArgs chk{};
+  chk.m = m;
+  fill_options(opt, chk);
+  if (chk.approx_basis && (!Cr || !aligned16(Cr))) return SSN_ERR_INVALID_ARGUMENT;   // full rotated Gram needs Cr
   if (!workspace || workspace_bytes < ssn_newton_workspace_bytes(batch, m) || !aligned16(workspace))
     return SSN_ERR_WORKSPACE;
   DualArgs a{};

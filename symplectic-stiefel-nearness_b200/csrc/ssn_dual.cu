@@ -30,9 +30,9 @@ namespace ssn {
 
 enum Mat {
   M_CE = 0, M_JE, M_W, M_WT, M_P, M_PT, M_Q, M_SR, M_SI, M_G, M_D, M_R, M_PP, M_HP, M_DL,
-  M_T1, M_T2, M_T3, M_X0, M_X1, M_X2
+  M_T1, M_T2, M_T3, M_X0, M_X1, M_X2, M_DEN
 };
-static_assert(M_X2 + 1 == kDualMats, "workspace matrix count");
+static_assert(M_DEN + 1 == kDualMats, "workspace matrix count");
 
 constexpr uint32_t C_ONE = coef_bit(0, 0, 0, 1);
 constexpr uint32_t C_SHARED_B = coef_bit(0, 0, 0, 1) | coef_bit(1, 1, 0, 1);
@@ -139,7 +139,9 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   const int region = imax(8 * slot, spd_region_doubles(m));
   double* red = smem + region;                // 2*kWarps doubles
   double* lam = red + 2 * kWarps;             // kMaxM doubles
-  double* xch = lam + kMaxM;                  // 8 doubles
+  double* pdg = lam + kMaxM;                  // kMaxM doubles: diag(P) (adaptive preconditioner)
+  double* sdg = pdg + kMaxM;                  // kMaxM doubles: diag(Sr)
+  double* xch = sdg + kMaxM;                  // 8 doubles
   int* flag = reinterpret_cast<int*>(xch + 8);
   double* Zs = smem;                          // this CTA's rows of the HVP outer product
   const int zld = m + 1;
@@ -193,6 +195,8 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   double* T2 = ws + (size_t)M_T2 * mm;
   double* T3 = ws + (size_t)M_T3 * mm;
   double* Kg = ws + (size_t)M_X0 * mm;        // K = I + trial trial, staged through L2 for CL = 2
+  double* Dn = ws + (size_t)M_DEN * mm;       // adaptive preconditioner denominators (this CTA's rows)
+  const bool adaptive = a.adaptive_precond != 0;
 
   auto store_to = [&](double* dst) {
     return [dst, m](int, int i, int j, double v) { dst[i * m + j] = v; };
@@ -386,10 +390,24 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
         slope = team.sum(sl);
       } else {
         // PCG (:142-161)
+        if (adaptive) {
+          // diagonals of P and Sr (all rows of Sr are visible after the residual's cluster sum)
+          for (int i = threadIdx.x; i < m; i += kThreads) {
+            pdg[i] = Pm[i * m + i];
+            sdg[i] = Sr[i * m + i];
+          }
+          __syncthreads();
+          SSN_FOR_IJ(team, m, {
+            double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * Pm[e] * Sr[e] + 2.0 * Qm[e] * Si[e];
+            if (!(dn > 0.0)) dn = lam[i] + lam[j];   // only off-diagonal entries matter; keep them positive
+            Dn[e] = i == j ? 1.0 : dn;
+          })
+        }
+        auto den = [&](int i, int j, int e) { return adaptive ? Dn[e] : lam[i] + lam[j]; };
         double rz = 0.0;
         SSN_FOR_IJ(team, m, {
           const double r = -G[e];
-          const double z = __ddiv_rn(r, lam[i] + lam[j]);
+          const double z = __ddiv_rn(r, den(i, j, e));
           Rr[e] = r;
           Dd[e] = 0.0;
           Pp[e] = z;
@@ -427,14 +445,14 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
             const double r = __dsub_rn(Rr[e], __dmul_rn(alpha, hp));
             Rr[e] = r;
             rn2 += r * r;
-            rz_next += r * __ddiv_rn(r, lam[i] + lam[j]);
+            rz_next += r * __ddiv_rn(r, den(i, j, e));
           })
           team.sum2(rn2, rz_next);
           const double rnorm = sqrt(rn2);
           if (!(rnorm > tol)) break;  // (:155-157)
           const double beta = rz_next / rz;
           SSN_FOR_IJ(team, m, {
-            Pp[e] = __dadd_rn(__ddiv_rn(Rr[e], lam[i] + lam[j]), __dmul_rn(beta, Pp[e]));
+            Pp[e] = __dadd_rn(__ddiv_rn(Rr[e], den(i, j, e)), __dmul_rn(beta, Pp[e]));
           })
           team.sync();
           rz = rz_next;
@@ -447,7 +465,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           ++n_fallback;
           double s2 = 0.0;
           SSN_FOR_IJ(team, m, {
-            const double z = __ddiv_rn(-G[e], lam[i] + lam[j]);
+            const double z = __ddiv_rn(-G[e], den(i, j, e));
             Dd[e] = z;
             s2 += G[e] * z;
           })
@@ -594,7 +612,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
 
 static size_t dual_smem_bytes(int MB) {
   const int region = imax(8 * slot_doubles(MB), spd_region_doubles(32 * MB));
-  return sizeof(double) * ((size_t)region + 2 * kWarps + kMaxM + 8) + 16;
+  return sizeof(double) * ((size_t)region + 2 * kWarps + 3 * kMaxM + 8) + 16;
 }
 
 static int sm_count() {

@@ -10,7 +10,7 @@
 namespace ssn {
 
 // Number of m x m FP64 matrices of per-instance dual workspace.
-constexpr int kDualMats = 21;
+constexpr int kDualMats = 22;
 
 struct DualArgs {
   int m;
@@ -29,13 +29,22 @@ struct DualArgs {
   int64_t* iterations;     // [B] out
   int32_t* status;         // [B] out
   int32_t* counters;       // [B,4] out: newton steps, hvps, trials, fallbacks (may be null)
-  // Approximate eigenbasis (split-precision form): the vectors only roughly
-  // diagonalise Cr/s.  The kernel then works with the full rotated Gram
-  // V^T (Cr/s) V in the sandwich and takes the preconditioner's lambda from its
-  // diagonal.  orthogonalize: first make V orthogonal to FP64 rounding with two
+  // Full rotated Gram: the kernel works with V^T (Cr/s) V in the sandwich
+  // instead of assuming it is exactly diag(lambda), and takes lambda from its
+  // diagonal.  Needed when the vectors only roughly diagonalise Cr/s (split
+  // form), and used with the adaptive preconditioner, where the iteration can
+  // pass near-singular I + i omega whose inverse would amplify the eigenbasis'
+  // rounding residual.  orthogonalize: first make V orthogonal to FP64 rounding with two
   // Newton-Schulz steps V <- V (3I - V^T V) / 2 (vectors from FP32 rotations).
   int approx_basis;
   int orthogonalize;
+  // Preconditioner of the CG (and of the fallback direction): 0 the reference's
+  // skew(R / (lambda_i + lambda_j)), exact for omega = 0; 1 the diagonal of the
+  // Hessian at the current omega in the working basis,
+  //   P_ii Sr_jj + P_jj Sr_ii - 2 P_ij Sr_ij + 2 Q_ij Si_ij,
+  // which equals lambda_i + lambda_j at omega = 0 and keeps CG short where
+  // omega is large (ill-conditioned targets).
+  int adaptive_precond;
 };
 
 size_t eigh_smem_bytes(int m);

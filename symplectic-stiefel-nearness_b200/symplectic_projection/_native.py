@@ -61,11 +61,12 @@ class Options(ctypes.Structure):
     _fields_ = [("max_newton", ctypes.c_int), ("max_cg", ctypes.c_int),
                 ("max_backtrack", ctypes.c_int), ("feas_tol", ctypes.c_double),
                 ("precision", ctypes.c_int), ("eig_sweeps", ctypes.c_int),
-                ("reserved", ctypes.c_int * 6)]
+                ("preconditioner", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
 
 
-# ssn_options.precision values (include/ssn.h)
+# ssn_options.precision / .preconditioner values (include/ssn.h)
 PRECISIONS = {"fp64": 0, "split": 1}
+PRECONDITIONERS = {"auto": 0, "eigenbasis": 1, "adaptive": 2}
 
 
 _lib = None
@@ -89,13 +90,16 @@ def load() -> ctypes.CDLL:
 
 
 def options(max_newton=100, max_cg=150, max_backtrack=40, feas_tol=1e-8, precision="fp64",
-            eig_sweeps=0) -> Options:
+            eig_sweeps=0, preconditioner="auto") -> Options:
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    if preconditioner not in PRECONDITIONERS:
+        raise ValueError(f"preconditioner must be one of {sorted(PRECONDITIONERS)}")
     opt = Options()
     load().ssn_default_options(ctypes.byref(opt))
     opt.max_newton, opt.max_cg, opt.max_backtrack, opt.feas_tol = max_newton, max_cg, max_backtrack, feas_tol
     opt.precision, opt.eig_sweeps = PRECISIONS[precision], eig_sweeps
+    opt.preconditioner = PRECONDITIONERS[preconditioner]
     return opt
 
 

@@ -62,7 +62,7 @@ def _pinned_like(T: torch.Tensor) -> torch.Tensor:
 @torch.no_grad()
 def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
              max_backtrack: int = MAX_BACKTRACK, feas_tol: float = FEAS_TOL,
-             precision: str = "fp64", eig_sweeps: int = 0,
+             precision: str = "fp64", eig_sweeps: int = 0, preconditioner: str = "auto",
              raise_on_failure: bool = False) -> SolveResult:
     """Device-resident solve with per-instance status.  T must be a CUDA tensor.
 
@@ -70,6 +70,10 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
     precision="split" takes the eigenbasis from ``eig_sweeps`` FP32 Jacobi
     sweeps (0: the library default) and works with the full rotated Gram, so
     it reaches the same dual optimum under the same acceptance bounds.
+    preconditioner="auto" uses the reference's eigenbasis preconditioner for the
+    FP64 form and the adaptive Hessian diagonal for the split form;
+    "eigenbasis" / "adaptive" force one.  The adaptive one keeps ill-conditioned
+    targets converging where the reference's CG saturates.
     """
     batch, n, m = _check_target(T)
     dev = N.require_cuda_f64(T)
@@ -83,7 +87,7 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
     lib = N.load()
     nbytes = lib.ssn_workspace_bytes(batch, n, m)
     ws = workspace(dev, nbytes)
-    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps)
+    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps, preconditioner)
     N.check(lib.ssn_solve(T.data_ptr(), X.data_ptr(), omega.data_ptr(), iterations.data_ptr(),
                           status.data_ptr(), batch, n, m, ws.data_ptr(), nbytes,
                           N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_solve")
@@ -257,7 +261,8 @@ def dual_batch(Cr, Ci, final=None, **options):
     ws = workspace(dev, nbytes)
     opt = N.options(options.get("max_newton", MAX_NEWTON), options.get("max_cg", MAX_CG),
                     options.get("max_backtrack", MAX_BACKTRACK), options.get("feas_tol", FEAS_TOL),
-                    options.get("precision", "fp64"), options.get("eig_sweeps", 0))
+                    options.get("precision", "fp64"), options.get("eig_sweeps", 0),
+                    options.get("preconditioner", "auto"))
     N.check(lib.ssn_dual(Cr.data_ptr(), Ci.data_ptr(), omega.data_ptr(), P.data_ptr(), Q.data_ptr(),
                          iterations.data_ptr(), status.data_ptr(), batch, m, ws.data_ptr(), nbytes,
                          N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_dual")

@@ -27,3 +27,29 @@ def gaussian_targets(n: int, k: int, count: int, case: int, base_seed: int = BAS
         gen = torch.Generator(device="cpu").manual_seed(base_seed + 1000 * case + j)
         out[j] = torch.randn(2 * n, 2 * k, dtype=torch.float64, generator=gen) / math.sqrt(2 * n)
     return out
+
+
+ILLCOND_SEED = 2026102500
+
+
+def illcond_targets(n: int, k: int, count: int, seed: int = ILLCOND_SEED,
+                    pin_memory: bool = False) -> torch.Tensor:
+    """Ill-conditioned stress targets T = U diag(s) V^T.
+
+    U (2n x 2k) and V (2k x 2k) have orthonormal columns from QR factors of
+    Gaussian matrices, s is log-uniform in [1e-2, 1e2], and every target is
+    scaled so that ||T||_F^2 = 2k.  One CPU generator seeded with ``seed``
+    draws all targets in order.  The reference's dual Newton-CG stalls on these
+    (its CG saturates and the Newton cap is reached); the adaptive
+    preconditioner keeps them converging.
+    """
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    out = torch.empty(count, 2 * n, 2 * k, dtype=torch.float64, pin_memory=pin_memory)
+    lo, hi = math.log(1e-2), math.log(1e2)
+    for j in range(count):
+        U, _ = torch.linalg.qr(torch.randn(2 * n, 2 * k, generator=gen, dtype=torch.float64))
+        V, _ = torch.linalg.qr(torch.randn(2 * k, 2 * k, generator=gen, dtype=torch.float64))
+        s = torch.exp(torch.empty(2 * k, dtype=torch.float64).uniform_(lo, hi, generator=gen))
+        T = U @ torch.diag(s) @ V.T
+        out[j] = T * (math.sqrt(2 * k) / torch.linalg.norm(T))
+    return out
