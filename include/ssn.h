@@ -74,23 +74,25 @@ typedef struct {
   double feas_tol;   /* 1e-8: an instance is done when residual < feas_tol / 2 */
   int precision;     /* SSN_PRECISION_FP64 (default) or SSN_PRECISION_SPLIT */
   int eig_sweeps;    /* split form: Jacobi sweeps of the rough eigenbasis (0 = default 3, max 24) */
-  int preconditioner; /* SSN_PRECOND_* (0 = automatic) */
+  int preconditioner; /* SSN_PRECOND_EIGENBASIS (default) or SSN_PRECOND_ADAPTIVE */
   int reserved[5];
 } ssn_options;
 
 /* CG preconditioner (ssn_options.preconditioner). */
 enum {
-  /* the reference's for the FP64 form, the adaptive one for the split form */
-  SSN_PRECOND_AUTO = 0,
   /* skew(R / (lambda_i + lambda_j)) in the eigenbasis of the scaled Gram: the
-   * reference's (dual_recommended_hvp.py:113-114), exact at omega = 0 */
-  SSN_PRECOND_EIGENBASIS = 1,
+   * reference's (dual_recommended_hvp.py:113-114), exact at omega = 0.  The
+   * default, in both precision forms. */
+  SSN_PRECOND_EIGENBASIS = 0,
   /* the diagonal of the Hessian at the current omega in the working basis,
    * P_ii Sr_jj + P_jj Sr_ii - 2 P_ij Sr_ij + 2 Q_ij Si_ij (lambda_i + lambda_j at
-   * omega = 0), with the full rotated Gram in the sandwich.  No counterpart in
-   * the reference: it keeps CG short on ill-conditioned targets, where the
-   * reference's preconditioner lets CG saturate and the Newton cap is reached. */
-  SSN_PRECOND_ADAPTIVE = 2
+   * omega = 0), with the full rotated Gram in the sandwich and the basis
+   * refined to FP64 orthogonality.  No counterpart in the reference: it keeps
+   * CG short on ill-conditioned targets, where the reference's preconditioner
+   * lets CG saturate and the Newton cap is reached.  It reaches the same dual
+   * optimum along another path, so on targets whose dual is very flat the
+   * result agrees with the reference's only to that flatness. */
+  SSN_PRECOND_ADAPTIVE = 1
 };
 
 /* Library version as 10000*major + 100*minor + patch. */

@@ -116,9 +116,12 @@ void fill_options(const ssn_options* opt, DualArgs& a) {
   a.max_backtrack = opt->max_backtrack;
   a.feas_tol = opt->feas_tol;
   const bool split = opt->precision == SSN_PRECISION_SPLIT;
-  a.adaptive_precond = opt->preconditioner == SSN_PRECOND_ADAPTIVE || (opt->preconditioner == SSN_PRECOND_AUTO && split);
+  a.adaptive_precond = opt->preconditioner == SSN_PRECOND_ADAPTIVE ? 1 : 0;
   a.approx_basis = (split || a.adaptive_precond) ? 1 : 0;    // full rotated Gram
-  a.orthogonalize = split ? 1 : 0;                            // FP32 rotations: refine V in FP64
+  // refine V to FP64 orthogonality with the full Gram: needed for FP32 rotations, and worth
+  // its four m x m products for FP64 ones too, whose ~1e-14 residue ill-conditioned targets
+  // (an inverse of norm ~1e2 in P + iQ) amplify into the primal's stationarity
+  a.orthogonalize = a.approx_basis;
 }
 
 bool split_form(const ssn_options* opt) { return opt && opt->precision == SSN_PRECISION_SPLIT; }
@@ -131,7 +134,7 @@ bool options_ok(const ssn_options* opt) {
          opt->feas_tol > 0.0 &&
          (opt->precision == SSN_PRECISION_FP64 || opt->precision == SSN_PRECISION_SPLIT) &&
          opt->eig_sweeps >= 0 && opt->eig_sweeps <= 24 &&
-         opt->preconditioner >= SSN_PRECOND_AUTO && opt->preconditioner <= SSN_PRECOND_ADAPTIVE;
+         (opt->preconditioner == SSN_PRECOND_EIGENBASIS || opt->preconditioner == SSN_PRECOND_ADAPTIVE);
 }
 
 // Eigenbasis of the scaled Gram for either precision form.

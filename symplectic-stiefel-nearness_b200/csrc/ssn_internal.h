@@ -34,8 +34,8 @@ struct DualArgs {
   // diagonal.  Needed when the vectors only roughly diagonalise Cr/s (split
   // form), and used with the adaptive preconditioner, where the iteration can
   // pass near-singular I + i omega whose inverse would amplify the eigenbasis'
-  // rounding residual.  orthogonalize: first make V orthogonal to FP64 rounding with two
-  // Newton-Schulz steps V <- V (3I - V^T V) / 2 (vectors from FP32 rotations).
+  // rounding residual.  orthogonalize: first make V orthogonal to FP64 rounding
+  // with two Newton-Schulz steps V <- V (3I - V^T V) / 2.
   int approx_basis;
   int orthogonalize;
   // Preconditioner of the CG (and of the fallback direction): 0 the reference's

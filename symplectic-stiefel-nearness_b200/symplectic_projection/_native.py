@@ -66,7 +66,7 @@ class Options(ctypes.Structure):
 
 # ssn_options.precision / .preconditioner values (include/ssn.h)
 PRECISIONS = {"fp64": 0, "split": 1}
-PRECONDITIONERS = {"auto": 0, "eigenbasis": 1, "adaptive": 2}
+PRECONDITIONERS = {"eigenbasis": 0, "adaptive": 1}
 
 
 _lib = None
@@ -90,7 +90,7 @@ def load() -> ctypes.CDLL:
 
 
 def options(max_newton=100, max_cg=150, max_backtrack=40, feas_tol=1e-8, precision="fp64",
-            eig_sweeps=0, preconditioner="auto") -> Options:
+            eig_sweeps=0, preconditioner="eigenbasis") -> Options:
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     if preconditioner not in PRECONDITIONERS:

@@ -62,7 +62,7 @@ def _pinned_like(T: torch.Tensor) -> torch.Tensor:
 @torch.no_grad()
 def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
              max_backtrack: int = MAX_BACKTRACK, feas_tol: float = FEAS_TOL,
-             precision: str = "fp64", eig_sweeps: int = 0, preconditioner: str = "auto",
+             precision: str = "fp64", eig_sweeps: int = 0, preconditioner: str = "eigenbasis",
              raise_on_failure: bool = False) -> SolveResult:
     """Device-resident solve with per-instance status.  T must be a CUDA tensor.
 
@@ -70,9 +70,8 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
     precision="split" takes the eigenbasis from ``eig_sweeps`` FP32 Jacobi
     sweeps (0: the library default) and works with the full rotated Gram, so
     it reaches the same dual optimum under the same acceptance bounds.
-    preconditioner="auto" uses the reference's eigenbasis preconditioner for the
-    FP64 form and the adaptive Hessian diagonal for the split form;
-    "eigenbasis" / "adaptive" force one.  The adaptive one keeps ill-conditioned
+    preconditioner="eigenbasis" (default) is the reference's; "adaptive" uses
+    the Hessian diagonal at the current omega, which keeps ill-conditioned
     targets converging where the reference's CG saturates.
     """
     batch, n, m = _check_target(T)
@@ -262,7 +261,7 @@ def dual_batch(Cr, Ci, final=None, **options):
     opt = N.options(options.get("max_newton", MAX_NEWTON), options.get("max_cg", MAX_CG),
                     options.get("max_backtrack", MAX_BACKTRACK), options.get("feas_tol", FEAS_TOL),
                     options.get("precision", "fp64"), options.get("eig_sweeps", 0),
-                    options.get("preconditioner", "auto"))
+                    options.get("preconditioner", "eigenbasis"))
     N.check(lib.ssn_dual(Cr.data_ptr(), Ci.data_ptr(), omega.data_ptr(), P.data_ptr(), Q.data_ptr(),
                          iterations.data_ptr(), status.data_ptr(), batch, m, ws.data_ptr(), nbytes,
                          N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_dual")

@@ -62,11 +62,6 @@ def test_adaptive_preconditioner_solves_illconditioned_targets(sp, illcond, prec
         assert O.passes(rec), rec
 
 
-def test_split_form_uses_the_adaptive_preconditioner_by_default(sp, illcond):
-    res = sp.solve_ex(illcond[0].cuda(), precision="split")
-    assert res.status.cpu().tolist() == [0, 0]
-
-
 @pytest.mark.parametrize("name", ["n64_k8_b4", "n100_k20_b2", "n192_k48_b2", "n96_k64_b1", "n64_k4_b2_illcond"])
 def test_adaptive_preconditioner_keeps_reference_solutions(sp, name):
     data = load_golden(name)
