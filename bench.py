@@ -31,11 +31,30 @@ sys.path.insert(0, str(ROOT / "symplectic-stiefel-nearness_b200"))
 
 METRIC = "solves/s, 64×(8192×96) batch, all pass r_F/r_G/δ checks: split-prec vs FP64"
 PRECISION_NOTE = {
-    "split": "split-precision form: FP32 Jacobi eigenbasis (re-orthogonalised in FP64) + FP64 Newton-CG, "
+    "split": "split-precision form: INT8 Ozaki Gram and recovery on tcgen05 (six digits, exact INT32 "
+             "accumulation), FP32 Jacobi eigenbasis re-orthogonalised in FP64, FP64 Newton-CG; "
              "FP64 in and out",
     "fp64": "fp64 (plain FP64 form)",
 }
 N_DEFAULT, K_DEFAULT, BATCH_DEFAULT = 4096, 48, 64
+# DRAM bytes (read + write) of the Newton kernel per target at n = 4096, k = 48, from one ncu
+# capture of 24 targets (dram__bytes_read.sum + dram__bytes_write.sum = 5.726 MB + 2.453 MB);
+# each target's state is private, so traffic scales with the number of targets.
+NEWTON_DRAM_BYTES_PER_TARGET_C2 = (5726464 + 2452736) / 24
+HBM_FALLBACK_GBS = 6650.0        # copy bandwidth of this GPU type when no measured figure is present
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) and where it came from."""
+    path = Path(__file__).resolve().parent / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        for key in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if isinstance(data.get(key), (int, float)):
+                return float(data[key]), "measured"
+    except (OSError, ValueError):
+        pass
+    return HBM_FALLBACK_GBS, "fallback"
 
 
 def parse():
@@ -244,6 +263,7 @@ def run_ours(args):
         e1.record(stream)
         e1.synchronize()
         peak = max(peak, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    hbm_gbs, hbm_src = hbm_peak()
 
     solve_bytes = lib.ssn_workspace_bytes(B, n, m)
     solve_ws = torch.empty(solve_bytes, dtype=torch.uint8, device=dev)
@@ -320,7 +340,7 @@ def run_ours(args):
                                         "algorithmic_flops": newton_flops}
         sw = sweeps.cpu()
         phases_out["eigh"]["jacobi_sweeps"] = {"max": int(sw.max()), "mean": float(sw.double().mean())}
-        phases_out["hbm_floor_ms"] = 48.0 * n * m * B / 6549.8e9 * 1e3
+        phases_out["hbm_floor_ms"] = 48.0 * n * m * B / (hbm_gbs * 1e9) * 1e3
         phases_out["note"] = ("phases timed one after another through the component entry points; the "
                               "full solve overlaps the split form's recovery digits with the eigen and "
                               "Newton phases")
@@ -338,10 +358,20 @@ def run_ours(args):
     dominant = max(per_launch, key=lambda kk: per_launch[kk][1])
     fl, ms = per_launch[dominant]
     achieved = (fl / (ms * 1e-3) / 1e12) if fl else None
+    traffic = None
+    if dominant == "newton" and (n, k) == (N_DEFAULT, K_DEFAULT):
+        traffic = NEWTON_DRAM_BYTES_PER_TARGET_C2 * B
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None, "kernel": dominant,
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic, "kernel": dominant,
                 "peak_source": "FP64 DMMA rate measured in this run (ssn_probe_fp64_mma); "
-                               "no FP64 figure in the driver's peak file"}
+                               "the peak file has no FP64 figure",
+                "traffic_note": "DRAM bytes per launch from an ncu capture of 24 targets, scaled by targets"}
+    # the whole solve against HBM: T read twice and X written once (48 n m bytes per target)
+    solve_bytes_alg = 48.0 * n * m * B
+    solve_hbm = {"bound": "hbm", "algorithmic_bytes": solve_bytes_alg,
+                 "achieved_gbs": solve_bytes_alg / (head["ms_step"] * 1e-3) / 1e9, "peak_gbs": hbm_gbs,
+                 "peak_source": hbm_src}
+    solve_hbm["frac"] = solve_hbm["achieved_gbs"] / hbm_gbs
     passed, worst, clocks, phases_out = head["passed"], head["worst"], head["clocks"], head["phases"]
     ms_step, value = head["ms_step"], head["value"]
     compare = None
@@ -399,7 +429,8 @@ def run_ours(args):
             "e2e": {"value": world * B / (e2e_step * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step,
                     "link": link},
-            "gpu_launches": head["launches"] * K, "roofline": roofline, "phases": phases_out}
+            "gpu_launches": head["launches"] * K, "roofline": roofline, "solve_hbm": solve_hbm,
+            "phases": phases_out}
     if compare:
         line.update(compare)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
