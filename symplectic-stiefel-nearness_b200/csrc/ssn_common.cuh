@@ -149,16 +149,29 @@ __device__ __forceinline__ void load_panel(double* slot, const double* ptr, int 
   }
 }
 
+// Doubles of one staged K-panel of an operand with `rows` (a multiple of 8) outer
+// rows, in either layout: K-minor rows x kMinorLd, or K-major kPanelK x frag_ld(rows).
+__host__ __device__ constexpr int panel_slot(int rows) {
+  return (rows * kMinorLd > kPanelK * frag_ld(rows)) ? rows * kMinorLd : kPanelK * frag_ld(rows);
+}
+
 // CTA-wide product engine (kThreads threads, warps on a 4x4 grid).
 //   out_o[r][c] = sum_{a,b} sign(o,a,b) * op(A_a)[r][:] . op(B_b)[:][c]
 // for r < R, c < N, contraction K, with R, N <= 128.  Each warp owns a
 // (WR*8) x (WC*8) tile; row passes of 4*WR*8 rows cover R.  Results are handed
-// to epi(o, r, c, value) for every valid (r, c).  smem: 2 stages x 4 slots of
-// `slot` doubles.  All threads must call it; it ends with __syncthreads().
-template <int WR, int WC, int NA, int NB, int NOUT, uint32_t COEF, class Epi>
-__device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (&B)[NB], int R, int N, int K,
-                                   double* smem, int slot, Epi& epi) {
+// to epi(o, r, c, value) for every valid (r, c).
+//
+// K-panels stream through ST stages of shared memory, each [A_0 A_1 B_0 B_1]
+// with slotA doubles per A slot (>= panel_slot of the rows of one pass) and
+// slotB per B slot (>= panel_slot(N padded to 8)): ST - 1 panels are in flight
+// while one is consumed, and one barrier per panel both publishes the landed
+// panel and retires the stage that the next copy overwrites.  All threads must
+// call it; it ends with __syncthreads().
+template <int WR, int WC, int NA, int NB, int NOUT, uint32_t COEF, int ST, class Epi>
+__device__ __forceinline__ void tile_product_staged(const MatOp (&A)[NA], const MatOp (&B)[NB], int R, int N,
+                                                    int K, double* smem, int slotA, int slotB, Epi& epi) {
   static_assert(NA >= 1 && NA <= 2 && NB >= 1 && NB <= 2 && NOUT >= 1 && NOUT <= 2, "engine arity");
+  static_assert(ST >= 2 && ST <= 4, "pipeline depth");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   const int wrow = warp >> 2, wcol = warp & 3;
@@ -166,6 +179,9 @@ __device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (
   const int npanel = cdiv(K, kPanelK);
   const int N_pad = round_up(N, 8);
   const int pldB = frag_ld(N_pad);
+  const int stage_sz = 2 * slotA + 2 * slotB;
+  auto a_slot = [&](int stage, int a) { return smem + stage * stage_sz + a * slotA; };
+  auto b_slot = [&](int stage, int b) { return smem + stage * stage_sz + 2 * slotA + b * slotB; };
 
   for (int r0 = 0; r0 < R; r0 += RP) {
     const int Rp = imin(RP, R - r0);
@@ -184,29 +200,33 @@ __device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (
       for (int a = 0; a < NA; ++a) {
         const bool kminor = !A[a].trans;
         const double* base = A[a].trans ? A[a].ptr + r0 : A[a].ptr + (size_t)r0 * A[a].ld;
-        load_panel(smem + (stage * 4 + a) * slot, base, A[a].ld, kminor, Rp, Rp_pad, pldA, k0, K);
+        load_panel(a_slot(stage, a), base, A[a].ld, kminor, Rp, Rp_pad, pldA, k0, K);
       }
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
         if (B[b].alias >= 0) continue;
         const bool kminor = B[b].trans;
-        load_panel(smem + (stage * 4 + 2 + b) * slot, B[b].ptr, B[b].ld, kminor, N, N_pad, pldB, k0, K);
+        load_panel(b_slot(stage, b), B[b].ptr, B[b].ld, kminor, N, N_pad, pldB, k0, K);
       }
       cp_async_commit();
     };
 
     const int row_base = wrow * WR * 8;
     const int col_base = wcol * WC * 8;
-    issue(0, 0);
+#pragma unroll
+    for (int sp = 0; sp < ST - 1; ++sp) {
+      if (sp < npanel) issue(sp, sp * kPanelK);
+      else cp_async_commit();
+    }
     for (int kp = 0; kp < npanel; ++kp) {
-      if (kp + 1 < npanel) {
-        issue((kp + 1) & 1, (kp + 1) * kPanelK);
-      } else {
-        cp_async_commit();
+      cp_async_wait<ST - 2>();      // this thread's copies of panel kp have landed
+      __syncthreads();              // everyone's have; every warp is done with panel kp - 1
+      {
+        const int nk = kp + ST - 1;  // refill the stage panel kp - 1 used
+        if (nk < npanel) issue(nk % ST, nk * kPanelK);
+        else cp_async_commit();
       }
-      cp_async_wait<1>();
-      __syncthreads();
-      const int stage = kp & 1;
+      const int stage = kp % ST;
       if (row_base < Rp && col_base < N) {
 #pragma unroll
         for (int ks = 0; ks < kPanelK / 4; ++ks) {
@@ -214,7 +234,7 @@ __device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (
           double af[NA][WR], bf[NB][WC];
 #pragma unroll
           for (int a = 0; a < NA; ++a) {
-            const double* s = smem + (stage * 4 + a) * slot;
+            const double* s = a_slot(stage, a);
 #pragma unroll
             for (int i = 0; i < WR; ++i) {
               // sub-tiles past the padded row extent are never read (they may lie past the slot)
@@ -224,8 +244,7 @@ __device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (
           }
 #pragma unroll
           for (int b = 0; b < NB; ++b) {
-            const int sl = B[b].alias >= 0 ? B[b].alias : 2 + b;
-            const double* s = smem + (stage * 4 + sl) * slot;
+            const double* s = B[b].alias >= 0 ? a_slot(stage, B[b].alias) : b_slot(stage, b);
             const int ld = B[b].alias >= 0 ? pldA : pldB;
             const bool kminor = B[b].alias >= 0 ? false : (B[b].trans != 0);
 #pragma unroll
@@ -255,9 +274,9 @@ __device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (
               }
         }
       }
-      __syncthreads();
     }
     cp_async_wait<0>();
+    __syncthreads();   // every warp is done with the panels: epilogues may write over the stages
     // epilogue
 #pragma unroll
     for (int o = 0; o < NOUT; ++o)
@@ -271,8 +290,15 @@ __device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (
             const int c = col_base + j * 8 + 2 * t + e;
             if (r < Rp && c < N) epi(o, r0 + r, c, acc[o][i][j][e]);
           }
-    __syncthreads();
+    __syncthreads();   // epilogue writes are visible; the stages are free for the next pass
   }
+}
+
+// Two stages of four equal slots of `slot` doubles (8 * slot doubles of smem).
+template <int WR, int WC, int NA, int NB, int NOUT, uint32_t COEF, class Epi>
+__device__ __forceinline__ void tile_product(const MatOp (&A)[NA], const MatOp (&B)[NB], int R, int N, int K,
+                                   double* smem, int slot, Epi& epi) {
+  tile_product_staged<WR, WC, NA, NB, NOUT, COEF, 2>(A, B, R, N, K, smem, slot, slot, epi);
 }
 
 // Warp-tile shape for bucket MB (mp <= 32*MB) and NOUT accumulator sets,

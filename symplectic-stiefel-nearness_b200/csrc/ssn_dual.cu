@@ -96,11 +96,22 @@ struct Team {
   }
 };
 
+// Panel staging of the Newton kernel's products: A slots hold the rows of one CTA
+// (half of m for CL = 2), B slots all m columns; as many stages (up to 4) as fit
+// in 200 KB, since the operands come from L2 and the panel latency must be hidden.
+__host__ __device__ constexpr int dual_slot_a(int MB, int CL) { return panel_slot(CL == 2 ? 16 * MB : 32 * MB); }
+__host__ __device__ constexpr int dual_slot_b(int MB) { return panel_slot(32 * MB); }
+__host__ __device__ constexpr int dual_stages(int MB, int CL) {
+  return imax(2, imin(4, 25600 / (2 * dual_slot_a(MB, CL) + 2 * dual_slot_b(MB))));
+}
+__host__ __device__ constexpr int dual_region_doubles(int MB, int CL) {
+  return imax(dual_stages(MB, CL) * (2 * dual_slot_a(MB, CL) + 2 * dual_slot_b(MB)), spd_region_doubles(32 * MB));
+}
+
 template <int MB, int CL>
 struct Dual {
   int m;
   double* smem;
-  int slot;
   int r0, rows;
 
   // rows [r0, r0 + rows) of sum_{a,b} +-op(A_a) op(B_b); epi gets global row indices
@@ -115,7 +126,8 @@ struct Dual {
     }
     const int off = r0;
     auto shifted = [&](int o, int i, int j, double v) { epi(o, i + off, j, v); };
-    ssn::tile_product<TL::WR, TL::WC, NA, NB, NOUT, COEF>(As, B, rows, m, m, smem, slot, shifted);
+    ssn::tile_product_staged<TL::WR, TL::WC, NA, NB, NOUT, COEF, dual_stages(MB, CL)>(
+        As, B, rows, m, m, smem, dual_slot_a(MB, CL), dual_slot_b(MB), shifted);
   }
 };
 
@@ -129,14 +141,52 @@ struct Dual {
       BODY                                                                            \
     }
 
+// The same element order, with every operand of a group of rows per warp
+// loaded before any element is used: load(i, j, e) returns the operands of
+// (i, j) (a scalar or a small struct), use(i, j, e, operands) computes and
+// stores.  The working matrices live in L2, and a loop that loads, stores and
+// loads again pays one L2 round trip per element; batching the loads pays one
+// per group.  The visiting order, and so every per-thread partial sum, is that
+// of SSN_FOR_IJ.
+template <int CPL, class Team_, class Load, class Use>
+__device__ __forceinline__ void each_ij(const Team_& tm, int m, Load&& load, Use&& use) {
+  using V = decltype(load(0, 0, 0));
+  // rows per group: about 18 doubles of operands per thread, so the group stays in registers
+  constexpr int QG = imax(1, imin(3, 6 / (int)(sizeof(V) / sizeof(double))));
+  const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+  for (int i0 = tm.r0 + warp; i0 < tm.r1; i0 += QG * kWarps) {
+    V v[QG][CPL];
+#pragma unroll
+    for (int q = 0; q < QG; ++q)
+#pragma unroll
+      for (int p = 0; p < CPL; ++p) {
+        // out-of-range slots load a valid element (never used), so every slot is defined
+        const int i = imin(i0 + q * kWarps, tm.r1 - 1), j = imin(lane + 32 * p, m - 1);
+        v[q][p] = load(i, j, i * m + j);
+      }
+#pragma unroll
+    for (int q = 0; q < QG; ++q)
+#pragma unroll
+      for (int p = 0; p < CPL; ++p) {
+        const int i = i0 + q * kWarps, j = lane + 32 * p;
+        if (i < tm.r1 && j < m) use(i, j, i * m + j, v[q][p]);
+      }
+  }
+}
+
+struct D2 { double x, y; };
+struct D3 { double x, y, z; };
+struct D4 { double x, y, z, w; };
+struct D5 { double x, y, z, w, u; };
+struct D6 { double x, y, z, w, u, d; };
+
 template <int MB, int CL>
 __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   extern __shared__ __align__(16) double smem[];
   const int m = a.m, mm = m * m;
   const int rank = CL == 1 ? 0 : (int)cg::this_cluster().block_rank();
   const int inst = blockIdx.x / CL;
-  const int slot = slot_doubles(MB);
-  const int region = imax(8 * slot, spd_region_doubles(m));
+  constexpr int region = dual_region_doubles(MB, CL);
   double* red = smem + region;                // 2*kWarps doubles
   double* lam = red + 2 * kWarps;             // kMaxM doubles
   double* pdg = lam + kMaxM;                  // kMaxM doubles: diag(P) (adaptive preconditioner)
@@ -162,7 +212,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
     Zpeer = cg::this_cluster().map_shared_rank(Zs, rank ^ 1);
     peer_r0 = imin(m, (rank ^ 1) * half);
   }
-  Dual<MB, CL> eng{m, smem, slot, team.r0, team.r1 - team.r0};
+  Dual<MB, CL> eng{m, smem, team.r0, team.r1 - team.r0};
   // Z(j, i) for any row j: this CTA's rows from local shared memory, the others from the peer's
   auto zval = [&](int j, int i) -> double {
     if (CL == 1 || (j >= team.r0 && j < team.r1)) return Zs[(j - team.r0) * zld + i];
@@ -235,10 +285,11 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       }
       V = Vin;                                  // == M_X1
     }
-    SSN_FOR_IJ(team, m, {
-      T1[e] = Ci[e] / s;
-      T3[e] = i < h ? V[(i + h) * m + j] : -V[(i - h) * m + j];
-    })
+    each_ij<MB>(team, m, [&](int i, int j, int e) { return D2{Ci[e], V[(i < h ? i + h : i - h) * m + j]}; },
+        [&](int i, int, int e, const D2& v) {
+          T1[e] = v.x / s;
+          T3[e] = i < h ? v.y : -v.y;
+        });
     team.sync();
     if (a.approx_basis) {
       double* Kt = ws + (size_t)M_X0 * mm;
@@ -295,15 +346,19 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
     // later pass relies on: precondition(r) = r / den and skew(w + t d) = w + t d
     // hold bit for bit for exactly skew r, w, d.
     const bool approx = a.approx_basis != 0;
-    SSN_FOR_IJ(team, m, {
-      const int et = j * m + i;
-      Ce[e] = (T1[e] - T1[et]) / 2;
-      Je[e] = ((Dl[e] - Dl[et]) / 2) / s;
-      Wm[e] = 0.0;
-      Pm[e] = (i == j) ? 1.0 : 0.0;
-      Qm[e] = 0.0;
-      if (!approx) Sr[e] = (i == j) ? lam[i] : 0.0;
-    })
+    each_ij<MB>(team, m,
+        [&](int i, int j, int e) {
+          const int et = j * m + i;
+          return D4{T1[e], T1[et], Dl[e], Dl[et]};
+        },
+        [&](int i, int j, int e, const D4& v) {
+          Ce[e] = (v.x - v.y) / 2;
+          Je[e] = ((v.z - v.w) / 2) / s;
+          Wm[e] = 0.0;
+          Pm[e] = (i == j) ? 1.0 : 0.0;
+          Qm[e] = 0.0;
+          if (!approx) Sr[e] = (i == j) ? lam[i] : 0.0;
+        });
     team.sync();
 
     const double sqrt_m = sqrt(static_cast<double>(m));
@@ -352,21 +407,26 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       // Sr = sym, Si = skew, gradient = Je - Si and its norm (:126-128)
       double gn2 = 0.0;
       if (step > 0) {
-        SSN_FOR_IJ(team, m, {
-          const int et = j * m + i;
-          Sr[e] = (T3[e] + T3[et]) / 2;
-          const double x = (Dl[e] - Dl[et]) / 2;
-          Si[e] = x;
-          const double gij = Je[e] - x;
-          G[e] = gij;
-          gn2 += gij * gij;
-        })
+        each_ij<MB>(team, m,
+            [&](int i, int j, int e) {
+              const int et = j * m + i;
+              return D5{T3[e], T3[et], Dl[e], Dl[et], Je[e]};
+            },
+            [&](int, int, int e, const D5& v) {
+              Sr[e] = (v.x + v.y) / 2;
+              const double x = (v.z - v.w) / 2;
+              Si[e] = x;
+              const double gij = v.u - x;
+              G[e] = gij;
+              gn2 += gij * gij;
+            });
       } else {
-        SSN_FOR_IJ(team, m, {
-          const double gij = Je[e] - Ce[e];
-          G[e] = gij;
-          gn2 += gij * gij;
-        })
+        each_ij<MB>(team, m, [&](int, int, int e) { return D2{Je[e], Ce[e]}; },
+            [&](int, int, int e, const D2& v) {
+              const double gij = v.x - v.y;
+              G[e] = gij;
+              gn2 += gij * gij;
+            });
       }
       const double gnorm = sqrt(team.sum(gn2));
       const double residual = gnorm * s / sqrt_m;
@@ -382,11 +442,12 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       if (step == 0) {
         // one preconditioner application solves H(E) = E L + L E exactly (:138-140)
         double sl = 0.0;
-        SSN_FOR_IJ(team, m, {
-          const double z = __ddiv_rn(-G[e], lam[i] + lam[j]);
-          Dd[e] = z;
-          sl += G[e] * z;
-        })
+        each_ij<MB>(team, m, [&](int, int, int e) { return G[e]; },
+            [&](int i, int j, int e, double gv) {
+              const double z = __ddiv_rn(-gv, lam[i] + lam[j]);
+              Dd[e] = z;
+              sl += gv * z;
+            });
         slope = team.sum(sl);
       } else {
         // PCG (:142-161)
@@ -397,22 +458,24 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
             sdg[i] = Sr[i * m + i];
           }
           __syncthreads();
-          SSN_FOR_IJ(team, m, {
-            double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * Pm[e] * Sr[e] + 2.0 * Qm[e] * Si[e];
-            if (!(dn > 0.0)) dn = lam[i] + lam[j];   // only off-diagonal entries matter; keep them positive
-            Dn[e] = i == j ? 1.0 : dn;
-          })
+          each_ij<MB>(team, m, [&](int, int, int e) { return D4{Pm[e], Sr[e], Qm[e], Si[e]}; },
+              [&](int i, int j, int e, const D4& v) {
+                double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * v.x * v.y + 2.0 * v.z * v.w;
+                if (!(dn > 0.0)) dn = lam[i] + lam[j];   // only off-diagonal entries matter; keep them positive
+                Dn[e] = i == j ? 1.0 : dn;
+              });
         }
         auto den = [&](int i, int j, int e) { return adaptive ? Dn[e] : lam[i] + lam[j]; };
         double rz = 0.0;
-        SSN_FOR_IJ(team, m, {
-          const double r = -G[e];
-          const double z = __ddiv_rn(r, den(i, j, e));
-          Rr[e] = r;
-          Dd[e] = 0.0;
-          Pp[e] = z;
-          rz += r * z;
-        })
+        each_ij<MB>(team, m, [&](int i, int j, int e) { return D2{G[e], den(i, j, e)}; },
+            [&](int, int, int e, const D2& v) {
+              const double r = -v.x;
+              const double z = __ddiv_rn(r, v.y);
+              Rr[e] = r;
+              Dd[e] = 0.0;
+              Pp[e] = z;
+              rz += r * z;
+            });
         rz = team.sum(rz);
         const double tol = fmin(fmax(sqrt(residual), 1e-8), 0.1) * gnorm;
         for (int it = 0; it < a.max_cg; ++it) {
@@ -434,41 +497,45 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           team.sync();
           ++n_hvp;
           double curv = 0.0;
-          SSN_FOR_IJ(team, m, { curv += Pp[e] * (zval(i, j) - zval(j, i)); })
+          each_ij<MB>(team, m, [&](int i, int j, int e) { return D3{Pp[e], zval(i, j), zval(j, i)}; },
+              [&](int, int, int, const D3& v) { curv += v.x * (v.y - v.z); });
           curv = team.sum(curv);
           if (!(curv > 0.0)) break;  // cg_active &= curvature > 0 (:152)
           const double alpha = rz / curv;
           double rn2 = 0.0, rz_next = 0.0;
-          SSN_FOR_IJ(team, m, {
-            const double hp = zval(i, j) - zval(j, i);
-            Dd[e] = __dadd_rn(Dd[e], __dmul_rn(alpha, Pp[e]));
-            const double r = __dsub_rn(Rr[e], __dmul_rn(alpha, hp));
-            Rr[e] = r;
-            rn2 += r * r;
-            rz_next += r * __ddiv_rn(r, den(i, j, e));
-          })
+          each_ij<MB>(team, m,
+              [&](int i, int j, int e) { return D6{zval(i, j), zval(j, i), Dd[e], Pp[e], Rr[e], den(i, j, e)}; },
+              [&](int, int, int e, const D6& v) {
+                const double hp = v.x - v.y;
+                Dd[e] = __dadd_rn(v.z, __dmul_rn(alpha, v.w));
+                const double r = __dsub_rn(v.u, __dmul_rn(alpha, hp));
+                Rr[e] = r;
+                rn2 += r * r;
+                rz_next += r * __ddiv_rn(r, v.d);
+              });
           team.sum2(rn2, rz_next);
           const double rnorm = sqrt(rn2);
           if (!(rnorm > tol)) break;  // (:155-157)
           const double beta = rz_next / rz;
-          SSN_FOR_IJ(team, m, {
-            Pp[e] = __dadd_rn(__ddiv_rn(Rr[e], den(i, j, e)), __dmul_rn(beta, Pp[e]));
-          })
+          each_ij<MB>(team, m, [&](int i, int j, int e) { return D3{Rr[e], den(i, j, e), Pp[e]}; },
+              [&](int, int, int e, const D3& v) { Pp[e] = __dadd_rn(__ddiv_rn(v.x, v.y), __dmul_rn(beta, v.z)); });
           team.sync();
           rz = rz_next;
         }
         double sl = 0.0;
-        SSN_FOR_IJ(team, m, { sl += G[e] * Dd[e]; })
+        each_ij<MB>(team, m, [&](int, int, int e) { return D2{G[e], Dd[e]}; },
+            [&](int, int, int, const D2& v) { sl += v.x * v.y; });
         slope = team.sum(sl);
         // non-descent fallback to the preconditioned gradient (:163-164)
         if (slope >= 0.0) {
           ++n_fallback;
           double s2 = 0.0;
-          SSN_FOR_IJ(team, m, {
-            const double z = __ddiv_rn(-G[e], den(i, j, e));
-            Dd[e] = z;
-            s2 += G[e] * z;
-          })
+          each_ij<MB>(team, m, [&](int i, int j, int e) { return D2{G[e], den(i, j, e)}; },
+              [&](int, int, int e, const D2& v) {
+                const double z = __ddiv_rn(-v.x, v.y);
+                Dd[e] = z;
+                s2 += v.x * z;
+              });
           slope = team.sum(s2);
         }
       }
@@ -479,12 +546,13 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
       for (int bt = 0; bt < a.max_backtrack; ++bt) {
         ++n_trial;
         double first = 0.0;
-        SSN_FOR_IJ(team, m, {
-          const double dl = __dmul_rn(t, Dd[e]);
-          Dl[e] = dl;
-          first += G[e] * dl;
-          Wt[e] = __dadd_rn(Wm[e], dl);      // == skew(omega + delta) for exactly skew omega, delta
-        })
+        each_ij<MB>(team, m, [&](int, int, int e) { return D3{Dd[e], G[e], Wm[e]}; },
+            [&](int, int, int e, const D3& v) {
+              const double dl = __dmul_rn(t, v.x);
+              Dl[e] = dl;
+              first += v.y * dl;
+              Wt[e] = __dadd_rn(v.z, dl);      // == skew(omega + delta) for exactly skew omega, delta
+            });
         first = team.sum(first);
         // K = I + trial trial, positive-definiteness test + inverse in shared memory
         double* Ks = smem;
@@ -610,8 +678,8 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   if constexpr (CL == 2) cg::this_cluster().sync();   // no CTA leaves while its peer may read its shared memory
 }
 
-static size_t dual_smem_bytes(int MB) {
-  const int region = imax(8 * slot_doubles(MB), spd_region_doubles(32 * MB));
+static size_t dual_smem_bytes(int MB, int CL) {
+  const int region = dual_region_doubles(MB, CL);
   return sizeof(double) * ((size_t)region + 2 * kWarps + 3 * kMaxM + 8) + 16;
 }
 
@@ -627,7 +695,7 @@ static int sm_count() {
 
 template <int MB, int CL>
 static cudaError_t launch_dual_mb(const DualArgs& args, int batch, cudaStream_t stream) {
-  const size_t smem = dual_smem_bytes(MB);
+  const size_t smem = dual_smem_bytes(MB, CL);
   cudaError_t err = cudaFuncSetAttribute(dual_kernel<MB, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;

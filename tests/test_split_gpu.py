@@ -64,7 +64,7 @@ def test_split_matches_reference_fixture(sp, name, manifest):
         assert O.passes(rec), rec
 
 
-@pytest.mark.parametrize("sweeps", [1, 2, 5, 12])
+@pytest.mark.parametrize("sweeps", [1, 2, 3, 5, 12])
 def test_split_sweep_count_does_not_change_the_solution(sp, sweeps):
     data = load_golden("n100_k20_b2")
     T = torch.from_numpy(data["T"]).cuda()
