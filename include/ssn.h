@@ -122,6 +122,26 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations,
               const ssn_options* opt, ssn_stream_t stream);
 
 /*
+ * Ragged batch: `count` targets of different shapes in one call.  Instance i is
+ * T_i [2 n[i], m[i]] row-major at T + t_offset[i] (offsets in doubles, even),
+ * its X_i at X + t_offset[i] and its omega_i [m[i], m[i]] at omega +
+ * w_offset[i]; iterations[i] and status[i] as in ssn_solve.  n, m, t_offset and
+ * w_offset are HOST arrays.  The instances are grouped by shape; every group is
+ * gathered into a contiguous batch, solved by the ssn_solve pipeline and
+ * scattered back, with the groups running concurrently on streams forked from
+ * (and joined back into) `stream`.  The plan goes to the device with one copy
+ * from pageable host memory, which waits for the work already on `stream`.
+ * Replaces a loop of symplectic_projection.solve calls, one per shape
+ * (dual_recommended_hvp.py:231-242).
+ */
+size_t ssn_ragged_workspace_bytes(int count, const int* n, const int* m);
+int ssn_solve_ragged(const double* T, double* X, double* omega, int64_t* iterations,
+                     int32_t* status, int count, const int* n, const int* m,
+                     const int64_t* t_offset, const int64_t* w_offset,
+                     void* workspace, size_t workspace_bytes,
+                     const ssn_options* opt, ssn_stream_t stream);
+
+/*
  * Gram products of T = [A; D]:  Cr = A^T A + D^T D,  Ci = A^T D - D^T A
  * (overwritten, not accumulated).  A, D are [batch, rows, m] with batch
  * strides ab_stride (elements, >= rows*m).  Replaces gram_add_

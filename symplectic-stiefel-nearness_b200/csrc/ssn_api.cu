@@ -151,49 +151,15 @@ cudaError_t eigenbasis(const ssn_options* opt, const double* Cr, double* values,
 
 }  // namespace
 
-extern "C" {
+namespace ssn {
 
-int ssn_version(void) { return kVersion; }
+size_t solve_workspace_bytes(int batch, int n, int m) { return solve_layout(batch, n, m).total; }
+bool solve_options_ok(const ssn_options* opt) { return options_ok(opt); }
 
-const char* ssn_status_string(int status) {
-  switch (status) {
-    case SSN_OK: return "ok";
-    case SSN_ERR_INVALID_ARGUMENT: return "invalid argument";
-    case SSN_ERR_CUDA: return "CUDA error";
-    case SSN_ERR_NEWTON_CAP: return "batched Newton iteration cap reached";
-    case SSN_ERR_LINE_SEARCH: return "batched line search found no descent step";
-    case SSN_ERR_NONFINITE: return "non-finite value in the iteration";
-    case SSN_ERR_EIGH: return "Jacobi eigensolver did not converge";
-    case SSN_ERR_WORKSPACE: return "workspace missing or too small";
-    case SSN_ERR_SCRATCH_LIMIT: return "problem exceeds the fixed scratch of the no-allocation entry point";
-    default: return "unknown status";
-  }
-}
-
-void ssn_default_options(ssn_options* opt) {
-  if (!opt) return;
-  memset(opt, 0, sizeof(*opt));
-  opt->max_newton = 100;
-  opt->max_cg = 150;
-  opt->max_backtrack = 40;
-  opt->feas_tol = 1e-8;
-}
-
-size_t ssn_workspace_bytes(int batch, int n, int m) {
-  if (!shape_ok(batch, m) || n < m / 2) return 0;
-  return solve_layout(batch, n, m).total;
-}
-
-int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status,
-              int batch, int n, int m, void* workspace, size_t workspace_bytes,
-              const ssn_options* opt, ssn_stream_t stream_) {
-  if (!shape_ok(batch, m) || n < m / 2 || !T || !X || !omega || !iterations || !status ||
-      !options_ok(opt))
-    return SSN_ERR_INVALID_ARGUMENT;
-  if (!aligned16(T) || !aligned16(X) || !aligned16(omega)) return SSN_ERR_INVALID_ARGUMENT;
+// Arguments checked by the caller (ssn_solve, ssn_solve_ragged).
+int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch,
+                int n, int m, void* workspace, const ssn_options* opt, cudaStream_t stream, int concurrent) {
   const SolveLayout L = solve_layout(batch, n, m);
-  if (!workspace || workspace_bytes < L.total || !aligned16(workspace)) return SSN_ERR_WORKSPACE;
-  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   char* ws = static_cast<char*>(workspace);
   double* Cr = reinterpret_cast<double*>(ws + L.cr);
   double* Ci = reinterpret_cast<double*>(ws + L.ci);
@@ -240,6 +206,7 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
   a.iterations = iterations;
   a.status = status;
   a.counters = nullptr;
+  a.concurrent = concurrent;
   e = launch_dual(a, batch, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   if (split) {
@@ -250,6 +217,54 @@ int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, in
     e = launch_recover(A, D, stride, Pf, Qf, X, X + (size_t)n * m, stride, batch, n, m, stream);
   }
   return cuda_status(e);
+}
+
+}  // namespace ssn
+
+extern "C" {
+
+int ssn_version(void) { return kVersion; }
+
+const char* ssn_status_string(int status) {
+  switch (status) {
+    case SSN_OK: return "ok";
+    case SSN_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case SSN_ERR_CUDA: return "CUDA error";
+    case SSN_ERR_NEWTON_CAP: return "batched Newton iteration cap reached";
+    case SSN_ERR_LINE_SEARCH: return "batched line search found no descent step";
+    case SSN_ERR_NONFINITE: return "non-finite value in the iteration";
+    case SSN_ERR_EIGH: return "Jacobi eigensolver did not converge";
+    case SSN_ERR_WORKSPACE: return "workspace missing or too small";
+    case SSN_ERR_SCRATCH_LIMIT: return "problem exceeds the fixed scratch of the no-allocation entry point";
+    default: return "unknown status";
+  }
+}
+
+void ssn_default_options(ssn_options* opt) {
+  if (!opt) return;
+  memset(opt, 0, sizeof(*opt));
+  opt->max_newton = 100;
+  opt->max_cg = 150;
+  opt->max_backtrack = 40;
+  opt->feas_tol = 1e-8;
+}
+
+size_t ssn_workspace_bytes(int batch, int n, int m) {
+  if (!shape_ok(batch, m) || n < m / 2) return 0;
+  return solve_layout(batch, n, m).total;
+}
+
+int ssn_solve(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status,
+              int batch, int n, int m, void* workspace, size_t workspace_bytes,
+              const ssn_options* opt, ssn_stream_t stream_) {
+  if (!shape_ok(batch, m) || n < m / 2 || !T || !X || !omega || !iterations || !status ||
+      !options_ok(opt))
+    return SSN_ERR_INVALID_ARGUMENT;
+  if (!aligned16(T) || !aligned16(X) || !aligned16(omega)) return SSN_ERR_INVALID_ARGUMENT;
+  if (!workspace || workspace_bytes < solve_layout(batch, n, m).total || !aligned16(workspace))
+    return SSN_ERR_WORKSPACE;
+  return solve_batch(T, X, omega, iterations, status, batch, n, m, workspace, opt,
+                     reinterpret_cast<cudaStream_t>(stream_), 0);
 }
 
 size_t gram_fp64_bytes(int batch, int rows, int m) { return sizeof(double) * gram_partial_doubles(batch, rows, m); }

@@ -721,7 +721,7 @@ static cudaError_t launch_dual_mb(const DualArgs& args, int batch, cudaStream_t 
 int dual_cluster_size(int batch, int m) { return (m >= 48 && 2 * batch <= sm_count()) ? 2 : 1; }
 
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
-  const bool two = dual_cluster_size(batch, args.m) == 2;
+  const bool two = dual_cluster_size(imax(batch, args.concurrent), args.m) == 2;
   switch (bucket_of(args.m)) {
     case 1: return launch_dual_mb<1, 1>(args, batch, stream);
     case 2: return two ? launch_dual_mb<2, 2>(args, batch, stream) : launch_dual_mb<2, 1>(args, batch, stream);

@@ -45,6 +45,9 @@ struct DualArgs {
   // which equals lambda_i + lambda_j at omega = 0 and keeps CG short where
   // omega is large (ill-conditioned targets).
   int adaptive_precond;
+  // Instances whose Newton kernels share the GPU at the same time (0: this batch
+  // alone).  A 2-CTA cluster per instance pays only while SMs would otherwise idle.
+  int concurrent;
 };
 
 size_t eigh_smem_bytes(int m);
@@ -58,6 +61,11 @@ cudaError_t launch_eigh_approx(const double* Cr, double* values, double* vectors
                                int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
                                int max_sweeps, bool fp32, cudaStream_t stream);
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
+// The whole uniform-batch solve (the body of ssn_solve) on one stream; `concurrent` as in DualArgs.
+int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch,
+                int n, int m, void* workspace, const ssn_options* opt, cudaStream_t stream, int concurrent);
+size_t solve_workspace_bytes(int batch, int n, int m);
+bool solve_options_ok(const ssn_options* opt);
 cudaError_t launch_probe_fp64_mma(double* sink, int iters, double* flops, cudaStream_t stream);
 cudaError_t launch_probe_s8_mma(const int8_t* A, const int8_t* B, int32_t* C, int n, int k, int* stall,
                                 cudaStream_t stream);

@@ -13,9 +13,9 @@ no CPU fallback.
 """
 from . import cholesky_inverse_kernel, gram_triangle_reflect, hvp_fused, recovery_fused
 from ._native import load as _load
-from .dual_recommended_hvp import solve, solve_ex
+from .dual_recommended_hvp import solve, solve_ex, solve_ragged
 
-__all__ = ["initialize_kernels", "solve", "solve_ex"]
+__all__ = ["initialize_kernels", "solve", "solve_ex", "solve_ragged"]
 
 _initialized = False
 

@@ -95,6 +95,66 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
     return SolveResult(X, omega, iterations, status)
 
 
+@torch.no_grad()
+def solve_ragged(targets, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
+                 max_backtrack: int = MAX_BACKTRACK, feas_tol: float = FEAS_TOL,
+                 precision: str = "fp64", eig_sweeps: int = 0, preconditioner: str = "eigenbasis",
+                 raise_on_failure: bool = True):
+    """Solve targets of different shapes in one call (ssn_solve_ragged).
+
+    ``targets`` is a sequence of float64 [2n_i, 2k_i] tensors, all on the host or all
+    on one CUDA device.  Returns (list of X_i, list of omega_i, iterations int64
+    [count], status int32 [count]) on the targets' device.  Each instance gets the
+    same result as solving it alone with ``solve``; with ``raise_on_failure`` a cap
+    on any instance raises RuntimeError for the whole call, as ``solve`` does.
+    """
+    targets = list(targets)
+    if not targets:
+        raise ValueError("no targets")
+    on_host = not targets[0].is_cuda
+    ns, ms = [], []
+    for t in targets:
+        if t.dim() != 2 or t.dtype != torch.float64 or t.is_cuda == on_host:
+            raise ValueError("targets must be 2-D float64 tensors, all on the host or all on one device")
+        rows, m = t.shape
+        if rows % 2 or m % 2 or m > 128 or rows // 2 < m // 2 or m == 0:
+            raise ValueError(f"target shape {tuple(t.shape)} is not [2n, 2k] with 1 <= k <= 64, n >= k")
+        ns.append(rows // 2)
+        ms.append(m)
+    dev = torch.device("cuda", torch.cuda.current_device()) if on_host else targets[0].device
+    flat = torch.cat([t.reshape(-1) for t in targets])
+    flat = flat.to(dev, non_blocking=False) if on_host else flat
+    count = len(targets)
+    t_off = [0] * count
+    w_off = [0] * count
+    tt = ww = 0
+    for i in range(count):
+        t_off[i], w_off[i] = tt, ww
+        tt += 2 * ns[i] * ms[i]
+        ww += ms[i] * ms[i]
+    X = torch.empty_like(flat)
+    omega = torch.empty(ww, dtype=torch.float64, device=dev)
+    iterations = torch.empty(count, dtype=torch.int64, device=dev)
+    status = torch.empty(count, dtype=torch.int32, device=dev)
+    c_int = N.ctypes.c_int * count
+    c_i64 = N.ctypes.c_int64 * count
+    n_arr, m_arr, t_arr, w_arr = c_int(*ns), c_int(*ms), c_i64(*t_off), c_i64(*w_off)
+    lib = N.load()
+    nbytes = lib.ssn_ragged_workspace_bytes(count, n_arr, m_arr)
+    ws = workspace(dev, nbytes)
+    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps, preconditioner)
+    N.check(lib.ssn_solve_ragged(flat.data_ptr(), X.data_ptr(), omega.data_ptr(), iterations.data_ptr(),
+                                 status.data_ptr(), count, n_arr, m_arr, t_arr, w_arr, ws.data_ptr(), nbytes,
+                                 N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_solve_ragged")
+    if raise_on_failure:
+        raise_for_status(status)
+    if on_host:
+        X, omega, iterations, status = X.cpu(), omega.cpu(), iterations.cpu(), status.cpu()
+    Xs = [X[t_off[i]:t_off[i] + 2 * ns[i] * ms[i]].view(2 * ns[i], ms[i]) for i in range(count)]
+    Ws = [omega[w_off[i]:w_off[i] + ms[i] * ms[i]].view(ms[i], ms[i]) for i in range(count)]
+    return Xs, Ws, iterations, status
+
+
 def raise_for_status(status: torch.Tensor) -> None:
     """Raise RuntimeError for the batch if any instance hit a cap (synchronises)."""
     codes = status.cpu().tolist()

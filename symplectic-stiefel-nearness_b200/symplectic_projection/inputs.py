@@ -53,3 +53,29 @@ def illcond_targets(n: int, k: int, count: int, seed: int = ILLCOND_SEED,
         T = U @ torch.diag(s) @ V.T
         out[j] = T * (math.sqrt(2 * k) / torch.linalg.norm(T))
     return out
+
+
+RAGGED_SEED = 2026102300
+RAGGED_N = (512, 1024, 2048, 4096, 8192)
+RAGGED_K = (8, 16, 24, 32, 48, 64)
+
+
+def ragged_shapes(count: int = 384, seed: int = RAGGED_SEED):
+    """(n, k) of each target of the ragged workload: n uniform over RAGGED_N and k
+    uniform over RAGGED_K, drawn by one CPU generator seeded with ``seed``."""
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    ni = torch.randint(0, len(RAGGED_N), (count,), generator=gen).tolist()
+    ki = torch.randint(0, len(RAGGED_K), (count,), generator=gen).tolist()
+    return [(RAGGED_N[a], RAGGED_K[b]) for a, b in zip(ni, ki)]
+
+
+def ragged_targets(count: int = 384, seed: int = RAGGED_SEED, shapes=None):
+    """Targets of the ragged workload: target j is N(0, 1/(2n_j)) of shape [2n_j, 2k_j]
+    from a CPU generator seeded with seed + 1 + j (the reference generator's rule,
+    with per-target seeds)."""
+    shapes = shapes if shapes is not None else ragged_shapes(count, seed)
+    out = []
+    for j, (n, k) in enumerate(shapes):
+        gen = torch.Generator(device="cpu").manual_seed(seed + 1 + j)
+        out.append(torch.randn(2 * n, 2 * k, dtype=torch.float64, generator=gen) / math.sqrt(2 * n))
+    return out

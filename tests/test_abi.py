@@ -76,3 +76,24 @@ def test_python_api_validates_on_host():
         sp.solve(torch.zeros(2, 7, 4, dtype=torch.float64))
     with pytest.raises(ValueError):
         sp.solve(torch.zeros(2, 2, 4, dtype=torch.float64))   # n < k
+
+
+def test_ragged_arguments_and_workspace_on_host(lib):
+    import ctypes
+    ints = lambda *v: (ctypes.c_int * len(v))(*v)
+    i64 = lambda *v: (ctypes.c_int64 * len(v))(*v)
+    n, m = ints(64, 100, 64), ints(8, 40, 8)
+    one = lib.ssn_ragged_workspace_bytes(1, ints(64), ints(8))
+    three = lib.ssn_ragged_workspace_bytes(3, n, m)
+    assert 0 < one < three
+    # two shape groups: at least the uniform workspaces of both plus gathered T, X and omega
+    floor = lib.ssn_workspace_bytes(2, 64, 8) + lib.ssn_workspace_bytes(1, 100, 40)
+    assert three >= floor + 8 * 2 * (2 * 2 * 64 * 8 + 2 * 100 * 40)
+    assert lib.ssn_ragged_workspace_bytes(2, ints(64, 8), ints(8, 20)) == 0          # n < k
+    assert lib.ssn_ragged_workspace_bytes(1, ints(64), ints(7)) == 0                 # odd m
+    t_off, w_off = i64(0, 1024, 9024), i64(0, 64, 1664)
+    args = (16, 16, 16, 16, 16, 3, n, m, t_off, w_off)
+    assert lib.ssn_solve_ragged(*args, 16, 8, None, None) == 7                       # workspace too small
+    assert lib.ssn_solve_ragged(16, 16, 16, 16, 16, 3, n, m, i64(0, 1025, 9024), w_off, 16, three,
+                                None, None) == 1                                     # odd (misaligned) offset
+    assert lib.ssn_solve_ragged(None, 16, 16, 16, 16, 3, n, m, t_off, w_off, 16, three, None, None) == 1

@@ -101,3 +101,15 @@ def test_reduced_protocol_on_the_device(tmp_path, precision):
     for item in s["cases"]:
         assert item["batch"]["speedups"]["dual_sequential"] > 1.0     # one batched call beats four single ones
     assert (tmp_path / "run" / "summary.json").exists() and (tmp_path / "run" / "raw.jsonl").exists()
+
+
+def test_ragged_workload_rule():
+    from symplectic_projection.inputs import RAGGED_K, RAGGED_N, ragged_shapes, ragged_targets
+    shapes = ragged_shapes(384)
+    assert len(shapes) == 384 and ragged_shapes(384) == shapes
+    assert {n for n, _ in shapes} == set(RAGGED_N) and {k for _, k in shapes} == set(RAGGED_K)
+    assert 1.2e9 < sum(2 * n * 2 * k * 8 for n, k in shapes) < 1.35e9         # about 1.25 GB of T
+    t = ragged_targets(3, shapes=[(64, 4), (32, 2), (64, 4)])
+    assert [tuple(x.shape) for x in t] == [(128, 8), (64, 4), (128, 8)] and not torch.equal(t[0], t[2])
+    g = torch.Generator().manual_seed(2026102300 + 1 + 2)
+    assert torch.equal(t[2], torch.randn(128, 8, dtype=torch.float64, generator=g) / math.sqrt(128))
