@@ -175,12 +175,13 @@ __device__ __forceinline__ double horner6(const uint32_t (&a)[kDigits]) {
 // Cr = A^T A + D^T D and G = A^T D over row chunks of n: one CTA per (row chunk,
 // group of 32 output columns, instance).  The MMA's M = 128 rows are the m
 // columns of T (zero-padded), N = 32 the CTA's output columns, K the rows of
-// the chunk, streamed in sub-tiles of 32 rows of A and 32 rows of D.  Every
-// sub-tile is sliced into digit planes (K-major, 64 K bytes per operand row:
-// A rows then D rows) in a 3-stage shared ring; one thread issues the 63 MMAs
-// of the sub-tile (21 digit pairs x {A^T A, D^T D, A^T D}) into 12 TMEM
-// accumulators (6 levels x {Cr, G}, 32 columns each) and commits them to the
-// stage's mbarrier, which releases the stage for the sub-tile three ahead.
+// the chunk, streamed in sub-tiles of 32 rows of A and 32 rows of D.  One warp
+// bulk-copies the FP64 rows of each sub-tile into a ring of up to three stages;
+// sixteen slicing warps turn a stage into digit planes (K-major, 64 K bytes per
+// operand row: A rows then D rows) in one of two digit stages; one thread
+// issues the sub-tile's 21 digit pairs x {A^T A, D^T D, A^T D} as 18 MMAs with
+// stacked B digits into 12 TMEM accumulators (6 levels x {Cr, G}, 32 columns
+// each) and commits them to the digit stage's mbarrier, which frees it.
 // Column scales are per (chunk, column), shared by A and D so that Cr's two
 // halves can share accumulators; a pre-pass computes them (and the per-row
 // scales the recovery uses).  Partials go to [B][chunk][2][m][m] and are summed
@@ -246,10 +247,10 @@ __global__ void __launch_bounds__(kScaleThreads)
 // waiter sees every phase of the mbarriers it waits on: a parity wait is only
 // unambiguous when the waiter has observed the previous phase (a consumer that
 // skipped phases could see a parity match one phase early).
-constexpr int kGSliceWarps = 8;
+constexpr int kGSliceWarps = 16;
 constexpr int kGSlicers = kGSliceWarps * 32;
-constexpr int kGMmaWarp = kGSliceWarps;                    // warp 8: MMA issuer
-constexpr int kGLoadWarp = kGSliceWarps + 1;               // warp 9: TMA producer
+constexpr int kGMmaWarp = kGSliceWarps;                    // warp 16: MMA issuer
+constexpr int kGLoadWarp = kGSliceWarps + 1;               // warp 17: TMA producer
 constexpr int kGThreads = kGSlicers + 64;
 constexpr int kGSub = 32;                                  // rows of A (and of D) per sub-tile
 constexpr int kGN = 32;                                    // output columns per CTA (MMA N)
@@ -583,10 +584,11 @@ cudaError_t launch_gram_ozaki(const double* A, const double* D, int64_t ab_strid
 // persistent over its tiles: MMA M = a 128-row tile, N = stacked digits of the
 // group's 64 B rows, K = 2m in 32-byte steps.  The prep kernel slices B once per
 // (instance, group) into the stacked, step-major layout the CTA bulk-loads in
-// one copy; sixteen slicing warps load W straight from global memory two steps
-// ahead of the step they slice; the MMA warp runs a tile's steps once the
-// epilogue warps have drained the previous tile's accumulators (six levels of
-// 64 columns: 384 TMEM columns).
+// one copy; the W digits, made once by the W-digit kernel in the same layout,
+// arrive one 24 KB bulk copy per (tile, K step) into a ring of up to four
+// stages; the MMA warp runs a tile's steps once the eight epilogue warps have
+// drained the previous tile's accumulators (six levels of 64 columns: 384 TMEM
+// columns).
 namespace {
 
 constexpr int kRM = 128;                                  // rows per tile (MMA M)
@@ -598,8 +600,9 @@ constexpr int kRBStep = oz::kDigits * kRW * kRK;          // 12288: stacked B di
 constexpr int kRStagesMax = 4;                            // digit-plane stages (bulk copies of W digits)
 constexpr int kRMmaWarp = 0;                              // warp 0: MMA issuer (lane 0), TMEM allocator
 constexpr int kRLoadWarp = 1;                             // warp 1: bulk copies of the W digit steps
-constexpr int kREpiWarp0 = 4;                             // warps 4-7: epilogue, TMEM lane quarter = warp % 4
-constexpr int kRThreads = 8 * 32;
+constexpr int kREpiWarp0 = 4;                             // warps 4-11: epilogue, TMEM lane quarter = warp % 4
+constexpr int kREpiWarps = 8;                             // two per lane quarter, one per 32-column half
+constexpr int kRThreads = (kREpiWarp0 + kREpiWarps) * 32;
 constexpr int kRSmemMax = 227 * 1024 - 1024;              // opt-in limit minus the static shared memory
 constexpr uint32_t kRSbo = (kRK / 16) * tc::kCoreBytes;    // 256
 constexpr uint32_t kRTmemCols = 512;                      // 6 x 64 = 384 used
@@ -609,11 +612,11 @@ __host__ __device__ inline int rec_steps(int m) { return cdiv(2 * m, kRK); }
 constexpr int kREpiLd = 9;                                // padded row stride (doubles) of the epilogue transpose
 constexpr int kREpiBuf = 32 * kREpiLd * 8;                // 2304 bytes per epilogue warp
 __host__ __device__ inline int rec_stages(int m) {
-  const int f = (kRSmemMax - rec_steps(m) * kRBStep - 4 * kREpiBuf) / kRAStage;
+  const int f = (kRSmemMax - rec_steps(m) * kRBStep - kREpiWarps * kREpiBuf) / kRAStage;
   return f > kRStagesMax ? kRStagesMax : f;
 }
 __host__ __device__ inline int rec_smem(int m) {
-  return rec_steps(m) * kRBStep + rec_stages(m) * kRAStage + 4 * kREpiBuf;
+  return rec_steps(m) * kRBStep + rec_stages(m) * kRAStage + kREpiWarps * kREpiBuf;
 }
 
 // B row o, column c (o < 2m, c < 2m): rows [P_o | Q_o] (Ur), [-Q_o' | P_o'] (Ui).
@@ -763,7 +766,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
   const int32_t* rexp = row_exp + (size_t)b * rows;
   uint8_t* bsm = smem;                                              // nks x kRBStep
   uint8_t* asm_ = smem + nks * kRBStep;                             // nst x kRAStage
-  double* ebuf = reinterpret_cast<double*>(asm_ + nst * kRAStage);  // 4 x kREpiBuf bytes
+  double* ebuf = reinterpret_cast<double*>(asm_ + nst * kRAStage);  // kREpiWarps x kREpiBuf bytes
   const double nan = __longlong_as_double(0x7FF8000000000000ll);
 
   if (tid < kRW) {
@@ -778,7 +781,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
       tc::mbar_init(&bar_dfree[s], 1);
     }
     tc::mbar_init(&bar_acc_full, 1);
-    tc::mbar_init(&bar_acc_free, 4);
+    tc::mbar_init(&bar_acc_free, kREpiWarps);
     s_err = 0;
   }
   if (warp == kRMmaWarp) tc::tmem_alloc(&tmem_slot, kRTmemCols);
@@ -830,8 +833,9 @@ __global__ void __launch_bounds__(kRThreads, 1)
       }
     }
   } else if (warp >= kREpiWarp0) {
-    // ---- epilogue warps: TMEM lane quarter (warp % 4); 64 output columns of 32 rows
+    // ---- epilogue warps: TMEM lane quarter (warp % 4), 32 of the 64 output columns, 32 rows
     const int ew = warp - kREpiWarp0, quarter = warp & 3;
+    const int c0 = (ew >> 2) * (kRW / 2);
     double* buf = ebuf + ew * (kREpiBuf / 8);
     const uint32_t tbase = tc::tmem_at(tmem, quarter * 32, 0);
     for (int it = 0; it < ntl; ++it) {
@@ -841,7 +845,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
       const int rr = quarter * 32 + lane, r = r0 + rr;
       const int e = r < rows ? __ldg(rexp + r) : oz::kExpMin;
       const double rinv = e == oz::kExpNonFinite ? nan : oz::pow2(e - 26);
-      for (int jc = 0; jc < kRW; jc += 8) {
+      for (int jc = c0; jc < c0 + kRW / 2; jc += 8) {
         uint32_t v[oz::kDigits][8];
         if (ok) {
 #pragma unroll
@@ -849,7 +853,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
 #pragma unroll
           for (int l = 0; l < oz::kDigits; ++l) tc::tmem_wait8(v[l]);
         }
-        if (jc + 8 == kRW) {                         // all of this tile's TMEM reads are done
+        if (jc + 8 == c0 + kRW / 2) {               // all of this warp's TMEM reads of the tile are done
           tc::fence_before_sync();
           __syncwarp();
           if (lane == 0) tc::mbar_arrive(&bar_acc_free);
