@@ -142,6 +142,26 @@ int ssn_solve_ragged(const double* T, double* X, double* omega, int64_t* iterati
                      const ssn_options* opt, ssn_stream_t stream);
 
 /*
+ * Gradient through the solve (the adjoint): given T [batch, 2n, m], the solve's
+ * omega [batch, m, m] and the loss gradients G = dL/dX [batch, 2n, m] and Gw =
+ * dL/d omega [batch, m, m] (either may be NULL), writes dT = dL/dT [batch, 2n, m].
+ * Implicit differentiation of the dual optimality condition at omega: one
+ * preconditioned CG solve with the solver's Hessian-vector product per instance
+ * (tolerance 1e-12 relative, at most max(opt->max_cg, 10 m) steps) and FP64
+ * tall-skinny products.  status[b]: 0 ok, 3 CG cap, 5 non-finite or I + omega^2
+ * not positive definite (dT of that instance is NaN); cg_iterations may be NULL.
+ * No counterpart in the reference, which solves under torch.no_grad
+ * (dual_recommended_hvp.py:231); its operators are the reference's HVP
+ * (hvp_fused.py:22-53), sandwich (dual_recommended_hvp.py:67-71) and recovery
+ * (recovery_fused.py:19-30).
+ */
+size_t ssn_adjoint_workspace_bytes(int batch, int n, int m);
+int ssn_adjoint(const double* T, const double* omega, const double* G, const double* Gw,
+                double* dT, int32_t* status, int32_t* cg_iterations, int batch, int n, int m,
+                void* workspace, size_t workspace_bytes, const ssn_options* opt,
+                ssn_stream_t stream);
+
+/*
  * Gram products of T = [A; D]:  Cr = A^T A + D^T D,  Ci = A^T D - D^T A
  * (overwritten, not accumulated).  A, D are [batch, rows, m] with batch
  * strides ab_stride (elements, >= rows*m).  Replaces gram_add_

@@ -369,3 +369,102 @@ def worst(records):
         vals = [r.get(key) for r in records]
         out[key] = max((float("inf") if v is None else v) for v in vals)
     return out
+
+
+# --------------------------------------------------------------------------
+# gradient through the solve (no counterpart in the reference, whose solve runs
+# under torch.no_grad, dual_recommended_hvp.py:231): three independent routes
+# --------------------------------------------------------------------------
+def _loss(T, G, Gw=None):
+    X, omega, _ = solve(T)
+    val = frob_inner(G, X)
+    if Gw is not None:
+        val = val + frob_inner(Gw, omega)
+    return val
+
+
+def adjoint_formula(T: torch.Tensor, G: torch.Tensor, Gw: torch.Tensor | None = None) -> torch.Tensor:
+    """dL/dT for L = <G, X*(T)> + <Gw, omega(T)>, by implicit differentiation of the dual.
+
+    Complex form: b = A + iD, g = G_top + i G_bottom, K = (I + i omega)^-1, S = K b^H b K.
+    omega solves Im(S) = J_m; differentiating, H(d omega) = Im(K dC K) with
+    H(E) = Z - Z^T, Z = Re(K E S) (the solver's HVP).  Then
+      Gamma = -skew(Im(K g^H b K)) + skew(Gw),  H mu = Gamma (dense solve here),
+      dL/db = g K + 2i b K mu K,  dL/dT = [Re; Im].
+    """
+    _, omega, _ = solve(T)
+    B, rows, m = T.shape
+    n = rows // 2
+    b = torch.complex(T[:, :n], T[:, n:])
+    g = torch.complex(G[:, :n], G[:, n:])
+    eye = torch.eye(m, dtype=torch.complex128)
+    K = torch.linalg.inv(eye + 1j * omega.to(torch.complex128))
+    S = K @ (b.mH @ b) @ K
+    Sr, Si = (S.real + S.real.mT) / 2, skew(S.imag)
+    P, Q = K.real, K.imag
+    R = K @ (g.mH @ b) @ K
+    Gamma = -skew(R.imag)
+    if Gw is not None:
+        Gamma = Gamma + skew(Gw)
+    iu = torch.triu_indices(m, m, 1)
+    p = iu.shape[1]
+    mu = torch.zeros(B, m, m, dtype=torch.float64)
+    for inst in range(B):
+        cols = []
+        for c in range(p):
+            E = torch.zeros(m, m, dtype=torch.float64)
+            E[iu[0, c], iu[1, c]] = 1.0
+            E[iu[1, c], iu[0, c]] = -1.0
+            HE = hvp(P[inst], Q[inst], Sr[inst], Si[inst], E)
+            cols.append(HE[iu[0], iu[1]])
+        Hm = torch.stack(cols, dim=1)
+        coef = torch.linalg.solve(Hm, Gamma[inst][iu[0], iu[1]])
+        mu[inst][iu[0], iu[1]] = coef
+        mu[inst][iu[1], iu[0]] = -coef
+    N = 2j * K @ mu.to(torch.complex128) @ K
+    grad = g @ K + b @ N
+    return torch.cat((grad.real, grad.imag), dim=-2)
+
+
+def adjoint_fd(T, G, Gw=None, direction=None, h=1e-6, seed=0):
+    """Central difference (L(T + hV) - L(T - hV)) / 2h along V (seeded Gaussian when None), per instance."""
+    if direction is None:
+        gen = torch.Generator().manual_seed(seed)
+        direction = torch.randn(T.shape, dtype=torch.float64, generator=gen)
+    return (_loss(T + h * direction, G, Gw) - _loss(T - h * direction, G, Gw)) / (2 * h), direction
+
+
+def adjoint_kkt(T: torch.Tensor, G: torch.Tensor) -> torch.Tensor:
+    """dL/dT for L = <G, X*(T)> from the dense KKT system of the primal problem.
+
+    Stationarity of 1/2 ||X - T||^2 + 1/2 <Lam, X^T J X - J_m> (Lam skew) is
+    F1 = X - T - J X Lam = 0, feasibility F2 = upper(X^T J X - J_m) = 0.  With
+    z = (X, upper(Lam)), dL/dT is the X block of w solving (dF/dz)^T w = (G, 0).
+    Small sizes only (dense (2nm + m(m-1)/2)^2 system).
+    """
+    X, _, _ = solve(T)
+    B, rows, m = T.shape
+    iu = torch.triu_indices(m, m, 1)
+    jm = swap_rows(torch.eye(m, dtype=torch.float64))
+    out = torch.empty_like(T)
+    for inst in range(B):
+        t, x = T[inst], X[inst]
+        jx = swap_rows(x)
+        lam = torch.linalg.lstsq(jx, x - t).solution
+        lam = skew(lam)
+        z0 = torch.cat((x.reshape(-1), lam[iu[0], iu[1]]))
+
+        def F(z, t=t):
+            xx = z[: rows * m].reshape(rows, m)
+            L = torch.zeros(m, m, dtype=torch.float64)
+            L = L.index_put((iu[0], iu[1]), z[rows * m:])
+            L = L - L.mT
+            f1 = xx - t - swap_rows(xx) @ L
+            f2 = (xx.mT @ swap_rows(xx) - jm)[iu[0], iu[1]]
+            return torch.cat((f1.reshape(-1), f2))
+
+        Jz = torch.autograd.functional.jacobian(F, z0)
+        rhs = torch.cat((G[inst].reshape(-1), torch.zeros(iu.shape[1], dtype=torch.float64)))
+        w = torch.linalg.solve(Jz.mT, rhs)
+        out[inst] = w[: rows * m].reshape(rows, m)
+    return out

@@ -43,6 +43,8 @@ constexpr uint32_t C_CPLX = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1) | coef_b
 // (P + iQ)(C + iE): out0 = P C - Q E, out1 = P E + Q C
 constexpr uint32_t C_SANDF = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 2) | coef_bit(1, 0, 1, 1) |
                              coef_bit(1, 1, 0, 1);
+// out0 = A0 B0 + A1 B1
+constexpr uint32_t C_SHARED_SUM = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1);
 
 // Warp-tile shape of a CL-way row split for bucket MB: each CTA computes at most
 // round_up(32*MB / CL, 8) rows of every m x m product.
@@ -728,6 +730,276 @@ cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
     case 3: return two ? launch_dual_mb<3, 2>(args, batch, stream) : launch_dual_mb<3, 1>(args, batch, stream);
     default: return two ? launch_dual_mb<4, 2>(args, batch, stream) : launch_dual_mb<4, 1>(args, batch, stream);
   }
+}
+
+// ---------------------------------------------------------------- adjoint (implicit gradient)
+// Per instance, in the original basis, with K = (I + i omega)^-1 = P + iQ,
+// C = Cr + i Ci = b^H b and M = Mr + i Mi = g^H b (b = A + iD, g = Ga + iGd):
+//   S = K C K,  Gamma = -skew(Im(K M K)) + skew(G_omega),
+//   H mu = Gamma by preconditioned CG, H(E) = Z - Z^T with Z = P E Sr - Q E Si
+//   (the reference's Hessian-vector product, hvp_fused.py:22-53, which is
+//   minus the Jacobian of Im(S) - J_m in omega),
+//   N = 2i K mu K,
+// and writes P, Q and Pn = Nr^T, Qn = -Ni^T, so that two recovery products give
+//   dL/dT = [Re; Im] (g K + b N)  (recover(G, P, Q) + recover(T, Pn, Qn)).
+// The CG's preconditioner is the diagonal of H in this basis,
+//   P_ii Sr_jj + P_jj Sr_ii - 2 P_ij Sr_ij + 2 Q_ij Si_ij.
+// One CTA per instance; every branch follows CTA-wide reductions, so all
+// threads take the same path.
+enum AdjMat { A_SR = 0, A_SI, A_DN, A_MU, A_R, A_PP, A_T1, A_T2, A_Y1, A_Y2 };
+static_assert(A_Y2 + 1 <= kAdjointMats, "adjoint workspace matrix count");
+
+template <int MB>
+__global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
+  extern __shared__ __align__(16) double smem[];
+  const int m = a.m, mm = m * m, inst = blockIdx.x;
+  constexpr int region = dual_region_doubles(MB, 1);
+  double* red = smem + region;                // 2*kWarps doubles
+  int* flag = reinterpret_cast<int*>(red + 2 * kWarps);
+  double* Zs = smem;                          // rows of the HVP outer product
+  const int zld = m + 1;
+  Team<1> team;
+  team.rank = 0;
+  team.r0 = 0;
+  team.r1 = m;
+  team.red = red;
+  team.xch = red;
+  team.xch_peer = red;
+  team.parity = 0;
+  Dual<MB, 1> eng{m, smem, 0, m};
+
+  double* ws = a.work + (size_t)inst * kAdjointMats * mm;
+  double* Sr = ws + (size_t)A_SR * mm;
+  double* Si = ws + (size_t)A_SI * mm;
+  double* Dn = ws + (size_t)A_DN * mm;
+  double* Mu = ws + (size_t)A_MU * mm;
+  double* Rr = ws + (size_t)A_R * mm;
+  double* Pp = ws + (size_t)A_PP * mm;
+  double* T1 = ws + (size_t)A_T1 * mm;
+  double* T2 = ws + (size_t)A_T2 * mm;
+  double* Y1 = ws + (size_t)A_Y1 * mm;
+  double* Y2 = ws + (size_t)A_Y2 * mm;
+  const double* W = a.omega + (size_t)inst * mm;
+  const double* Cr = a.Cr + (size_t)inst * mm;
+  const double* Ci = a.Ci + (size_t)inst * mm;
+  const double* Mr = a.Mr + (size_t)inst * mm;
+  const double* Mi = a.Mi + (size_t)inst * mm;
+  const double* Gw = a.Gw ? a.Gw + (size_t)inst * mm : nullptr;
+  double* Pm = a.P + (size_t)inst * mm;
+  double* Qm = a.Q + (size_t)inst * mm;
+  double* Pn = a.Pn + (size_t)inst * mm;
+  double* Qn = a.Qn + (size_t)inst * mm;
+  int status = SSN_INSTANCE_CONVERGED;
+  int iters = 0;
+
+  // P = (I + omega omega)^-1 with the positive-definiteness test, Q = -omega P
+  {
+    double* Ks = smem;
+    const int mp16 = round_up(m, 16), kld = frag_ld(mp16);
+    MatOp A[1] = {op_n(W, m)};
+    MatOp B[1] = {op_n(W, m)};
+    auto epi = [&](int, int i, int j, double v) { Ks[i * kld + j] = (i == j ? 1.0 : 0.0) + v; };
+    eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+    for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {
+      const int i = e / mp16, j = e - i * mp16;
+      if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const bool valid = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
+    if (valid) {
+      SSN_FOR_IJ(team, m, { Pm[e] = Ks[i * kld + j]; })
+    } else {
+      status = SSN_INSTANCE_NONFINITE;
+    }
+    __syncthreads();
+  }
+  if (status == SSN_INSTANCE_CONVERGED) {
+    {
+      MatOp A[1] = {op_n(W, m)};
+      MatOp B[1] = {op_n(Pm, m)};
+      auto epi = [&](int, int i, int j, double v) { Qm[i * m + j] = -v; };
+      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+    }
+    __syncthreads();
+    // Y = K C, then S = Y K (Sr symmetric, Si antisymmetric parts)
+    {
+      MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
+      MatOp B[2] = {op_n(Cr, m), op_n(Ci, m)};
+      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Y1 : Y2)[i * m + j] = v; };
+      eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
+    }
+    __syncthreads();
+    {
+      MatOp A[2] = {op_n(Y1, m), op_n(Y2, m)};
+      MatOp B[2] = {op_n(Pm, m), op_n(Qm, m)};
+      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T2)[i * m + j] = v; };
+      eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
+    }
+    __syncthreads();
+    each_ij<MB>(team, m,
+        [&](int i, int j, int e) {
+          const int et = j * m + i;
+          return D4{T1[e], T1[et], T2[e], T2[et]};
+        },
+        [&](int, int, int e, const D4& v) {
+          Sr[e] = (v.x + v.y) / 2;
+          Si[e] = (v.z - v.w) / 2;
+        });
+    __syncthreads();
+    // Y = K M, then Im(Y K) = Y1 Q + Y2 P
+    {
+      MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
+      MatOp B[2] = {op_n(Mr, m), op_n(Mi, m)};
+      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Y1 : Y2)[i * m + j] = v; };
+      eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
+    }
+    __syncthreads();
+    {
+      MatOp A[2] = {op_n(Y1, m), op_n(Y2, m)};
+      MatOp B[2] = {op_n(Qm, m), op_n(Pm, m)};
+      auto epi = [&](int, int i, int j, double v) { T2[i * m + j] = v; };
+      eng.template mul<2, 2, 1, C_SHARED_SUM>(A, B, epi);
+    }
+    __syncthreads();
+    // Gamma = -skew(Im(K M K)) + skew(G_omega) (exactly antisymmetric), preconditioner,
+    // CG start: mu = 0, r = Gamma, p = r / den
+    for (int i = threadIdx.x; i < m; i += kThreads) {
+      red[2 * kWarps + 16 + i] = Pm[i * m + i];
+    }
+    double gn2 = 0.0, rz = 0.0;
+    {
+      double* pdg = red + 2 * kWarps + 16;              // diag(P) then diag(Sr), staged in shared memory
+      double* sdg = pdg + kMaxM;
+      for (int i = threadIdx.x; i < m; i += kThreads) sdg[i] = Sr[i * m + i];
+      __syncthreads();
+      each_ij<MB>(team, m,
+          [&](int i, int j, int e) {
+            const int et = j * m + i;
+            return D6{T2[e], T2[et], Gw ? Gw[e] : 0.0, Gw ? Gw[et] : 0.0, Sr[e], Qm[e] * Si[e]};
+          },
+          [&](int i, int j, int e, const D6& v) {
+            const double g = ((v.y - v.x) + (v.z - v.w)) / 2;
+            double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * Pm[e] * v.u + 2.0 * v.d;
+            if (!(dn > 0.0)) dn = 1.0;
+            if (i == j) dn = 1.0;
+            Dn[e] = dn;
+            Rr[e] = g;
+            Mu[e] = 0.0;
+            const double z = g / dn;
+            Pp[e] = z;
+            gn2 += g * g;
+            rz += g * z;
+          });
+    }
+    team.sum2(gn2, rz);
+    const double gnorm = sqrt(gn2);
+    if (!isfinite(gnorm) || !isfinite(rz)) status = SSN_INSTANCE_NONFINITE;
+    double rnorm = gnorm;
+    const double stop = a.tol * gnorm;
+    while (status == SSN_INSTANCE_CONVERGED && rnorm > stop) {
+      if (iters >= a.max_cg) {
+        status = SSN_INSTANCE_NEWTON_CAP;
+        break;
+      }
+      ++iters;
+      {
+        MatOp A[1] = {op_n(Pp, m)};
+        MatOp B[2] = {op_n(Sr, m), op_n(Si, m)};
+        auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T2)[i * m + j] = v; };
+        eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
+      }
+      __syncthreads();
+      {
+        MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
+        MatOp B[2] = {op_n(T1, m), op_n(T2, m)};
+        auto epi = [&](int, int i, int j, double v) { Zs[i * zld + j] = v; };
+        eng.template mul<2, 2, 1, C_DIFF>(A, B, epi);
+      }
+      __syncthreads();
+      double curv = 0.0;
+      each_ij<MB>(team, m, [&](int i, int j, int e) { return D3{Pp[e], Zs[i * zld + j], Zs[j * zld + i]}; },
+          [&](int, int, int, const D3& v) { curv += v.x * (v.y - v.z); });
+      curv = team.sum(curv);
+      if (!(curv > 0.0)) {            // H is positive definite at a strict dual optimum
+        status = isfinite(curv) ? SSN_INSTANCE_NEWTON_CAP : SSN_INSTANCE_NONFINITE;
+        break;
+      }
+      const double alpha = rz / curv;
+      double rn2 = 0.0, rz_next = 0.0;
+      each_ij<MB>(team, m,
+          [&](int i, int j, int e) { return D6{Zs[i * zld + j], Zs[j * zld + i], Mu[e], Pp[e], Rr[e], Dn[e]}; },
+          [&](int, int, int e, const D6& v) {
+            Mu[e] = v.z + alpha * v.w;
+            const double r = v.u - alpha * (v.x - v.y);
+            Rr[e] = r;
+            rn2 += r * r;
+            rz_next += r * (r / v.d);
+          });
+      team.sum2(rn2, rz_next);
+      rnorm = sqrt(rn2);
+      const double beta = rz_next / rz;
+      rz = rz_next;
+      each_ij<MB>(team, m, [&](int, int, int e) { return D3{Rr[e], Dn[e], Pp[e]}; },
+          [&](int, int, int e, const D3& v) { Pp[e] = v.x / v.y + beta * v.z; });
+      __syncthreads();
+    }
+    // N = 2i K mu K: U = [P mu, Q mu]; K mu K = (U1 P - U2 Q) + i (U1 Q + U2 P)
+    {
+      MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
+      MatOp B[1] = {op_n(Mu, m)};
+      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Y1 : Y2)[i * m + j] = v; };
+      eng.template mul<2, 1, 2, C_SHARED_B>(A, B, epi);
+    }
+    __syncthreads();
+    {
+      MatOp A[2] = {op_n(Y1, m), op_n(Y2, m)};
+      MatOp B[2] = {op_n(Pm, m), op_n(Qm, m)};
+      // Nr = -2 Im(K mu K), Ni = 2 Re(K mu K); Pn = Nr^T, Qn = -Ni^T
+      auto epi = [&](int o, int i, int j, double v) {
+        if (o == 0) Qn[j * m + i] = -2.0 * v;
+        else Pn[j * m + i] = -2.0 * v;
+      };
+      eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
+    }
+  }
+  if (status != SSN_INSTANCE_CONVERGED) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < mm; e += kThreads) {
+      Pn[e] = NAN;
+      Qn[e] = NAN;
+    }
+  }
+  if (threadIdx.x == 0) {
+    a.status[inst] = status;
+    if (a.cg_iters) a.cg_iters[inst] = iters;
+  }
+}
+
+size_t adjoint_smem_bytes(int m) {
+  const int MB = bucket_of(m);
+  const int region = MB == 1 ? dual_region_doubles(1, 1) : MB == 2 ? dual_region_doubles(2, 1)
+                   : MB == 3 ? dual_region_doubles(3, 1) : dual_region_doubles(4, 1);
+  return sizeof(double) * ((size_t)region + 2 * kWarps + 16 + 2 * kMaxM) + 16;
+}
+
+cudaError_t launch_adjoint(const AdjointArgs& args, int batch, cudaStream_t stream) {
+  const size_t smem = adjoint_smem_bytes(args.m);
+  cudaError_t err = cudaSuccess;
+#define SSN_ADJ_CASE(MBV)                                                                              \
+  case MBV:                                                                                            \
+    err = cudaFuncSetAttribute(adjoint_kernel<MBV>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                               static_cast<int>(smem));                                               \
+    if (err != cudaSuccess) return err;                                                                \
+    adjoint_kernel<MBV><<<batch, kThreads, smem, stream>>>(args);                                      \
+    break;
+  switch (bucket_of(args.m)) {
+    SSN_ADJ_CASE(1)
+    SSN_ADJ_CASE(2)
+    SSN_ADJ_CASE(3)
+    SSN_ADJ_CASE(4)
+  }
+#undef SSN_ADJ_CASE
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- SPD inverse component

@@ -143,6 +143,78 @@ cudaError_t launch_gram(const double* A, const double* D, int64_t ab_stride, dou
   return cudaGetLastError();
 }
 
+// Cross Gram of two tall-skinny pairs (the adjoint's g^H b): Mr = Ga^T A + Gd^T D,
+// Mi = Ga^T D - Gd^T A, row-split like the Gram; partials [B][splits][2][m][m].
+constexpr uint32_t C_XMR = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1);
+constexpr uint32_t C_XMI = coef_bit(0, 0, 1, 1) | coef_bit(0, 1, 0, 2);
+
+template <int MB>
+__global__ void __launch_bounds__(kThreads, 1)
+    cross_gram_kernel(const double* __restrict__ Ga, const double* __restrict__ Gd, int64_t g_stride,
+                      const double* __restrict__ A, const double* __restrict__ D, int64_t ab_stride,
+                      double* __restrict__ partial, int rows, int m, int chunk, int splits) {
+  extern __shared__ __align__(16) double smem[];
+  const int s = blockIdx.x, b = blockIdx.y;
+  const int mm = m * m;
+  const int r0 = s * chunk;
+  const int K = imin(rows, r0 + chunk) - r0;
+  double* out = partial + ((size_t)b * splits + s) * 2 * mm;
+  using TL = Tile<MB, 1>;
+  MatOp Aop[2] = {op_t(Ga + (size_t)b * g_stride + (size_t)r0 * m, m),
+                  op_t(Gd + (size_t)b * g_stride + (size_t)r0 * m, m)};
+  MatOp Bop[2] = {op_n(A + (size_t)b * ab_stride + (size_t)r0 * m, m),
+                  op_n(D + (size_t)b * ab_stride + (size_t)r0 * m, m)};
+  auto epi_r = [&](int, int i, int j, double v) { out[i * m + j] = v; };
+  auto epi_i = [&](int, int i, int j, double v) { out[(size_t)mm + i * m + j] = v; };
+  tile_product<TL::WR, TL::WC, 2, 2, 1, C_XMR>(Aop, Bop, m, m, K, smem, slot_doubles(MB), epi_r);
+  tile_product<TL::WR, TL::WC, 2, 2, 1, C_XMI>(Aop, Bop, m, m, K, smem, slot_doubles(MB), epi_i);
+}
+
+// Fixed-order sum of the cross Gram's split partials.
+__global__ void cross_gram_finalize_kernel(const double* __restrict__ partial, double* __restrict__ Mr,
+                                           double* __restrict__ Mi, int m, int splits) {
+  const int b = blockIdx.y, mm = m * m;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= mm) return;
+  const double* p = partial + (size_t)b * splits * 2 * mm;
+  double sr = 0.0, si = 0.0;
+  for (int s = 0; s < splits; ++s) {
+    sr += p[(size_t)s * 2 * mm + e];
+    si += p[(size_t)s * 2 * mm + mm + e];
+  }
+  Mr[(size_t)b * mm + e] = sr;
+  Mi[(size_t)b * mm + e] = si;
+}
+
+cudaError_t launch_cross_gram(const double* Ga, const double* Gd, int64_t g_stride, const double* A,
+                              const double* D, int64_t ab_stride, double* Mr, double* Mi, int batch, int rows,
+                              int m, double* partial, cudaStream_t stream) {
+  const GramSplit gs = gram_split(batch, rows);
+  const int MB = bucket_of(m);
+  const size_t smem = sizeof(double) * 8 * (size_t)slot_doubles(MB);
+  dim3 grid(gs.splits, batch);
+  cudaError_t err = cudaSuccess;
+#define SSN_XGRAM_CASE(MBV)                                                                          \
+  case MBV:                                                                                          \
+    err = cudaFuncSetAttribute(cross_gram_kernel<MBV>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                               static_cast<int>(smem));                                             \
+    if (err != cudaSuccess) return err;                                                              \
+    cross_gram_kernel<MBV><<<grid, kThreads, smem, stream>>>(Ga, Gd, g_stride, A, D, ab_stride,      \
+                                                             partial, rows, m, gs.chunk, gs.splits); \
+    break;
+  switch (MB) {
+    SSN_XGRAM_CASE(1)
+    SSN_XGRAM_CASE(2)
+    SSN_XGRAM_CASE(3)
+    SSN_XGRAM_CASE(4)
+  }
+#undef SSN_XGRAM_CASE
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  cross_gram_finalize_kernel<<<dim3(cdiv(m * m, 128), batch), 128, 0, stream>>>(partial, Mr, Mi, m, gs.splits);
+  return cudaGetLastError();
+}
+
 // rows per recovery CTA: WR limited so 2 outputs x WR x WC x 2 <= 36 doubles
 template <int MB>
 struct RecTile {

@@ -50,6 +50,31 @@ struct DualArgs {
   int concurrent;
 };
 
+// Adjoint of the solve (implicit gradient), one CTA per instance.
+constexpr int kAdjointMats = 10;
+struct AdjointArgs {
+  int m, max_cg;
+  double tol;              // CG stops at ||r|| <= tol ||Gamma||
+  const double* Cr;        // [B,m,m] b^H b, real and imaginary parts
+  const double* Ci;
+  const double* Mr;        // [B,m,m] g^H b
+  const double* Mi;
+  const double* omega;     // [B,m,m] the solve's multiplier (original basis)
+  const double* Gw;        // [B,m,m] dL/d omega, or null
+  double* work;            // [B, kAdjointMats, m, m]
+  double* P;               // [B,m,m] out: K = P + iQ
+  double* Q;
+  double* Pn;              // [B,m,m] out: recovery operands of b N
+  double* Qn;
+  int32_t* status;         // [B] out
+  int32_t* cg_iters;       // [B] out (may be null)
+};
+cudaError_t launch_adjoint(const AdjointArgs& args, int batch, cudaStream_t stream);
+// Mr = Ga^T A + Gd^T D, Mi = Ga^T D - Gd^T A (row-split partials summed in a fixed order).
+cudaError_t launch_cross_gram(const double* Ga, const double* Gd, int64_t g_stride, const double* A,
+                              const double* D, int64_t ab_stride, double* Mr, double* Mi, int batch, int rows,
+                              int m, double* partial, cudaStream_t stream);
+
 size_t eigh_smem_bytes(int m);
 size_t eigh_workspace_bytes(int batch, int m);
 cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, double* scale,

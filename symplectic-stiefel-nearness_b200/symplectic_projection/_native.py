@@ -28,6 +28,8 @@ PROTOTYPES = {
     "ssn_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_ragged_workspace_bytes": (_SZ, [_I, _P, _P]),
     "ssn_solve_ragged": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _SZ, _P, _P]),
+    "ssn_adjoint_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "ssn_adjoint": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_gram_workspace_bytes": (_SZ, [_I, _I, _I]),
     "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_gram_noalloc_scratch_bytes": (_SZ, []),

@@ -97,3 +97,12 @@ def test_ragged_arguments_and_workspace_on_host(lib):
     assert lib.ssn_solve_ragged(16, 16, 16, 16, 16, 3, n, m, i64(0, 1025, 9024), w_off, 16, three,
                                 None, None) == 1                                     # odd (misaligned) offset
     assert lib.ssn_solve_ragged(None, 16, 16, 16, 16, 3, n, m, t_off, w_off, 16, three, None, None) == 1
+
+
+def test_adjoint_arguments_on_host(lib):
+    a = lib.ssn_adjoint_workspace_bytes(8, 32, 8)
+    assert a > 0 and lib.ssn_adjoint_workspace_bytes(8, 32, 7) == 0 and lib.ssn_adjoint_workspace_bytes(0, 32, 8) == 0
+    assert lib.ssn_adjoint(16, 16, None, None, 16, 16, None, 8, 32, 8, 16, 8, None, None) == 7   # workspace
+    assert lib.ssn_adjoint(None, 16, None, None, 16, 16, None, 8, 32, 8, 16, a, None, None) == 1  # no T
+    assert lib.ssn_adjoint(16, 16, 8, None, 16, 16, None, 8, 32, 8, 16, a, None, None) == 1      # misaligned G
+    assert lib.ssn_adjoint(16, 16, None, None, 16, 16, None, 8, 2, 8, 16, a, None, None) == 1     # n < k

@@ -94,3 +94,17 @@ def test_adaptive_preconditioner_converges_where_the_reference_stalls():
         O.solve(T, preconditioner="eigenbasis")
     X, W, it = O.solve(T, preconditioner="adaptive")
     assert all(O.passes(r) for r in O.inspect_output(T, X))
+
+
+def test_adjoint_routes_agree_on_cpu():
+    """The dual closed-form adjoint equals the dense primal KKT adjoint and finite differences."""
+    T, _ = O.make_inputs(12, 2, 0, 2)
+    g = torch.Generator().manual_seed(4)
+    G = torch.randn(T.shape, dtype=torch.float64, generator=g)
+    Gw = torch.randn(2, 4, 4, dtype=torch.float64, generator=g)
+    a = O.adjoint_formula(T, G)
+    k = O.adjoint_kkt(T, G)
+    assert float(torch.linalg.vector_norm(a - k) / torch.linalg.vector_norm(k)) < 1e-10
+    fd, V = O.adjoint_fd(T, G, Gw, h=1e-6, seed=2)
+    ad = (O.adjoint_formula(T, G, Gw) * V).sum(dim=(-2, -1))
+    assert float(((ad - fd).abs() / fd.abs()).max()) < 1e-6
