@@ -72,9 +72,10 @@ def parse():
     p.add_argument("--precision", choices=["split", "fp64", "both"], default="both",
                    help="form timed for `value` (split when both; the FP64 form is then reported beside it)")
     p.add_argument("--eig-sweeps", type=int, default=0, help="split form: Jacobi sweeps (0 = library default)")
-    p.add_argument("--workload", choices=["uniform", "ragged"], default="uniform",
+    p.add_argument("--workload", choices=["uniform", "ragged", "adjoint"], default="uniform",
                    help="uniform: the --batch x (2n x 2k) batch; ragged: the 384-target mixed-shape batch "
-                        "through ssn_solve_ragged (one GPU)")
+                        "through ssn_solve_ragged; adjoint: solve + gradient of <G, X*(T)> for 64 targets "
+                        "of n = 2048, k = 32 (one GPU)")
     return p.parse_args()
 
 
@@ -544,12 +545,91 @@ def run_ragged(args):
     return 0 if passed else 1
 
 
+def run_adjoint(args):
+    """Differentiation workload: 64 targets, n = 2048, k = 32, L = <G, X*(T)> with G ~ N(0, 1) (seed
+    2026102199); one step = ssn_solve + ssn_adjoint (dL/dT), both device-resident."""
+    import torch
+    import symplectic_projection as sp
+    from symplectic_projection import _native as N
+    from symplectic_projection.certify import certify
+    from symplectic_projection.inputs import case_index, gaussian_targets
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    sp.initialize_kernels()
+    lib = N.load()
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    precision = "split" if args.precision == "both" else args.precision
+    B, n, k = 64, 2048, 32
+    m = 2 * k
+    T = gaussian_targets(n, k, B, case_index(n, k)).to(dev)
+    gen = torch.Generator().manual_seed(2026102199)
+    G = torch.randn(B, 2 * n, m, dtype=torch.float64, generator=gen).to(dev)
+    X, dT = torch.empty_like(T), torch.empty_like(T)
+    omega = torch.empty(B, m, m, dtype=torch.float64, device=dev)
+    iters = torch.empty(B, dtype=torch.int64, device=dev)
+    status = torch.empty(B, dtype=torch.int32, device=dev)
+    astat = torch.empty(B, dtype=torch.int32, device=dev)
+    acg = torch.empty(B, dtype=torch.int32, device=dev)
+    sbytes, abytes = lib.ssn_workspace_bytes(B, n, m), lib.ssn_adjoint_workspace_bytes(B, n, m)
+    ws_s = torch.empty(sbytes, dtype=torch.uint8, device=dev)
+    ws_a = torch.empty(abytes, dtype=torch.uint8, device=dev)
+    opt = N.options(precision=precision, eig_sweeps=args.eig_sweeps)
+
+    def forward():
+        N.check(lib.ssn_solve(T.data_ptr(), X.data_ptr(), omega.data_ptr(), iters.data_ptr(), status.data_ptr(),
+                              B, n, m, ws_s.data_ptr(), sbytes, N.ctypes.byref(opt), sh), "ssn_solve")
+
+    def backward():
+        N.check(lib.ssn_adjoint(T.data_ptr(), omega.data_ptr(), G.data_ptr(), None, dT.data_ptr(), astat.data_ptr(),
+                                acg.data_ptr(), B, n, m, ws_a.data_ptr(), abytes, None, sh), "ssn_adjoint")
+
+    for _ in range(max(3, args.warmup)):
+        forward()
+        backward()
+    torch.cuda.synchronize(dev)
+    K = max(1, min(args.steps, 100))
+    sampler = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+    sampler.start()
+    time.sleep(0.3)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for _ in range(K):
+        forward()
+    ev[1].record(stream)
+    for _ in range(K):
+        backward()
+    ev[2].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]) / K, ev[1].elapsed_time(ev[2]) / K
+    cert = certify(T, X)
+    passed = bool(cert["passed"].all()) and bool((status == 0).all()) and bool((astat == 0).all())
+    passed = passed and bool(torch.isfinite(dT).all())
+    step = fwd_ms + bwd_ms
+    line = {"metric": "forward+backward solves/s, 64 x (4096 x 64) batch, dL/dT of <G, X*(T)> by the adjoint",
+            "value": B / (step * 1e-3), "unit": "solves/s", "n_gpus": 1, "steps": K,
+            "warmup": max(3, args.warmup), "ms_per_step": step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded N(0,1/(2n)) targets, G ~ N(0,1)",
+            "config": {"workload": "64 x (4096 x 64) FP64 targets, n=2048, k=32, forward solve + adjoint",
+                       "precision": PRECISION_NOTE[precision] + "; adjoint FP64",
+                       "inputs": "T and G resident in HBM", "parallelism": "replicas x1"},
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+            "adjoint_cg_iterations": {"max": int(acg.max()), "mean": float(acg.double().mean())},
+            "all_pass": passed, "clocks": clocks, "gpu_launches": K * ((9 if precision == "split" else 6) + 8)}
+    print(json.dumps(line))
+    return 0 if passed else 1
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "ragged":
         return run_ragged(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 
