@@ -88,26 +88,40 @@ constexpr int kDefaultEigSweeps = 1;
 
 // A side stream forked from the caller's stream with events (and joined back the
 // same way), so work that only depends on the inputs can overlap later kernels.
-// Stream-capture safe: the fork and join are event record / wait pairs.  The
-// stream and events are created per call and released once their work is done.
+// The stream and its two events are created once per host thread and device and
+// kept: nothing is created or destroyed inside a call, so a call can be captured
+// into a CUDA graph (the fork and join become graph edges).  Calls from one
+// thread share the stream; the events order each call's side work correctly.
 struct SideStream {
   cudaStream_t stream = nullptr;
   cudaEvent_t forked = nullptr, done = nullptr;
   cudaError_t fork(cudaStream_t parent) {
-    cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&forked, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventRecord(forked, parent);
+    struct Pool {
+      cudaStream_t stream = nullptr;
+      cudaEvent_t forked = nullptr, done = nullptr;
+    };
+    constexpr int kMaxDevices = 64;
+    thread_local Pool pool[kMaxDevices];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    Pool& p = pool[dev];
+    if (!p.stream) {
+      e = cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.forked, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+    stream = p.stream;
+    forked = p.forked;
+    done = p.done;
+    e = cudaEventRecord(forked, parent);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, forked, 0);
     return e;
   }
   cudaError_t record() { return cudaEventRecord(done, stream); }
   cudaError_t join(cudaStream_t parent) { return cudaStreamWaitEvent(parent, done, 0); }
-  ~SideStream() {
-    if (done) cudaEventDestroy(done);
-    if (forked) cudaEventDestroy(forked);
-    if (stream) cudaStreamDestroy(stream);
-  }
 };
 
 void fill_options(const ssn_options* opt, DualArgs& a) {
