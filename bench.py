@@ -72,10 +72,14 @@ def parse():
     p.add_argument("--precision", choices=["split", "fp64", "both"], default="both",
                    help="form timed for `value` (split when both; the FP64 form is then reported beside it)")
     p.add_argument("--eig-sweeps", type=int, default=0, help="split form: Jacobi sweeps (0 = library default)")
-    p.add_argument("--workload", choices=["uniform", "ragged", "adjoint"], default="uniform",
+    p.add_argument("--feas-tol", type=float, default=1e-8,
+                   help="Newton stopping tolerance (residual < feas_tol / 2), as the reference's FEAS_TOL")
+    p.add_argument("--workload", choices=["uniform", "ragged", "adjoint", "illcond"], default="uniform",
                    help="uniform: the --batch x (2n x 2k) batch; ragged: the 384-target mixed-shape batch "
                         "through ssn_solve_ragged; adjoint: solve + gradient of <G, X*(T)> for 64 targets "
-                        "of n = 2048, k = 32 (one GPU)")
+                        "of n = 2048, k = 32; illcond: the ill-conditioned stress batch, 256 targets of "
+                        "n = 16384, k = 64, split forward with the adaptive preconditioner plus the adjoint "
+                        "(one GPU)")
     return p.parse_args()
 
 
@@ -622,6 +626,104 @@ def run_adjoint(args):
     return 0 if passed else 1
 
 
+def run_illcond(args):
+    """Ill-conditioned stress: 256 targets T = U diag(s) V^T of 32768 x 128 (s log-uniform in [1e-2, 1e2],
+    ||T||_F^2 = 2k), split-precision forward with the adaptive preconditioner, then the adjoint of
+    <G, X*(T)>; one step = ssn_solve + ssn_adjoint."""
+    import torch
+    import symplectic_projection as sp
+    from symplectic_projection import _native as N
+    from symplectic_projection.certify import certify
+    from symplectic_projection.inputs import illcond_targets
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    sp.initialize_kernels()
+    lib = N.load()
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    B = args.batch if args.batch != BATCH_DEFAULT else 256
+    n, k = 16384, 64
+    m = 2 * k
+    t0 = time.perf_counter()
+    T = illcond_targets(n, k, B).to(dev)
+    gen_s = time.perf_counter() - t0
+    gen = torch.Generator().manual_seed(2026102599)
+    G = torch.randn(B, 2 * n, m, dtype=torch.float64, generator=gen).to(dev)
+    X, dT = torch.empty_like(T), torch.empty_like(T)
+    omega = torch.empty(B, m, m, dtype=torch.float64, device=dev)
+    iters = torch.empty(B, dtype=torch.int64, device=dev)
+    status = torch.empty(B, dtype=torch.int32, device=dev)
+    astat = torch.empty(B, dtype=torch.int32, device=dev)
+    acg = torch.empty(B, dtype=torch.int32, device=dev)
+    sbytes, abytes = lib.ssn_workspace_bytes(B, n, m), lib.ssn_adjoint_workspace_bytes(B, n, m)
+    ws_s = torch.empty(sbytes, dtype=torch.uint8, device=dev)
+    ws_a = torch.empty(abytes, dtype=torch.uint8, device=dev)
+    precision = "split" if args.precision == "both" else args.precision
+    opt = N.options(feas_tol=args.feas_tol, precision=precision, eig_sweeps=args.eig_sweeps,
+                    preconditioner="adaptive")
+
+    def forward():
+        N.check(lib.ssn_solve(T.data_ptr(), X.data_ptr(), omega.data_ptr(), iters.data_ptr(), status.data_ptr(),
+                              B, n, m, ws_s.data_ptr(), sbytes, N.ctypes.byref(opt), sh), "ssn_solve")
+
+    def backward():
+        N.check(lib.ssn_adjoint(T.data_ptr(), omega.data_ptr(), G.data_ptr(), None, dT.data_ptr(), astat.data_ptr(),
+                                acg.data_ptr(), B, n, m, ws_a.data_ptr(), abytes, None, sh), "ssn_adjoint")
+
+    W = max(1, min(args.warmup, 2))
+    for _ in range(W):
+        forward()
+        backward()
+    torch.cuda.synchronize(dev)
+    K = max(1, min(args.steps, 5))
+    sampler = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+    sampler.start()
+    time.sleep(0.3)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for _ in range(K):
+        forward()
+    ev[1].record(stream)
+    for _ in range(K):
+        backward()
+    ev[2].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]) / K, ev[1].elapsed_time(ev[2]) / K
+    st = status.cpu()
+    worst = {"feasibility": 0.0, "stationarity": 0.0, "delta": 0.0}
+    passed_n, failing = 0, []
+    for c0 in range(0, B, 32):                       # certify in slices (bounded extra memory)
+        cert = certify(T[c0:c0 + 32], X[c0:c0 + 32])
+        passed_n += int(cert["passed"].sum())
+        for key in worst:
+            worst[key] = max(worst[key], float(cert[key].max()))
+        for j in (~cert["passed"]).nonzero().flatten().tolist():
+            failing.append({"instance": c0 + j, "status": int(st[c0 + j]), "newton_iterations": int(iters[c0 + j]),
+                            **{key: float(cert[key][j]) for key in worst}})
+    passed = passed_n == B and bool((st == 0).all()) and bool((astat == 0).all()) and bool(torch.isfinite(dT).all())
+    step = fwd_ms + bwd_ms
+    line = {"metric": "forward+backward solves/s, ill-conditioned 256 x (32768 x 128) batch, all pass r_F/r_G/δ checks",
+            "value": B / (step * 1e-3), "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: T = U diag(s) V^T, U, V from QR of seeded Gaussians, s log-uniform in [1e-2, 1e2]",
+            "config": {"workload": f"{B} x ({2 * n} x {m}) ill-conditioned FP64 targets, n={n}, k={k}, "
+                                   f"{8 * B * 2 * n * m / 1e9:.1f} GB of T",
+                       "precision": PRECISION_NOTE[precision] + "; adaptive CG preconditioner; adjoint FP64",
+                       "inputs": "T and G resident in HBM", "parallelism": "replicas x1",
+                       "generation_s": gen_s},
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+            "newton_iterations": {"max": int(iters.max()), "mean": float(iters.double().mean())},
+            "status_counts": {str(c): int((st == c).sum()) for c in st.unique().tolist()},
+            "instances_passing": passed_n, "failing": failing[:8], "feas_tol": args.feas_tol,
+            "adjoint_cg_iterations": {"max": int(acg.max()), "mean": float(acg.double().mean())},
+            "all_pass": passed, "worst": worst, "clocks": clocks,
+            "gpu_launches": K * ((9 if precision == "split" else 6) + 8)}
+    print(json.dumps(line))
+    return 0 if passed else 1
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -630,6 +732,8 @@ def main():
         return run_ragged(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "illcond":
+        return run_illcond(args)
     return run_ours(args)
 
 
