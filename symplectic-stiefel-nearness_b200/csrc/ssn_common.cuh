@@ -366,6 +366,72 @@ __device__ __forceinline__ void smem_product(int R, int N, int K, const double* 
   }
 }
 
+// One 16 x 16 block (rows r0.., columns c0..) of op(A)[R x 16] * op(B)[16 x N],
+// handed to fn(i, j, value); the same DMMA sequence as smem_product's blocks.
+template <bool AT, bool BT, class Fn>
+__device__ __forceinline__ void smem_block16(int r0, int c0, const double* A, int lda, const double* B, int ldb,
+                                             Fn&& fn) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  double acc[2][2][2] = {};
+#pragma unroll
+  for (int k = 0; k < 16; k += 4) {
+    double af[2], bf[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int r = r0 + 8 * i + g;
+      af[i] = AT ? A[(k + t) * lda + r] : A[r * lda + k + t];
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int c = c0 + 8 * j + g;
+      bf[j] = BT ? B[c * ldb + k + t] : B[(k + t) * ldb + c];
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) fn(r0 + 8 * i + g, c0 + 8 * j + 2 * t + e, acc[i][j][e]);
+}
+
+// Rank-16 update out(i, j) = X[i][:16] . U[:16][j] over an mp x mp square (mp = 32 WT),
+// one (8 WT) x (8 WT) tile per warp of a 4 x 4 warp grid (kThreads threads): WT^2
+// independent accumulators per warp, and each 8x8 fragment sees the same DMMA
+// sequence as in smem_product, so the results are the same bits.
+template <int WT, class Fn>
+__device__ __forceinline__ void smem_rank16_tiled(const double* X, int ldx, const double* U, int ldu, Fn&& fn) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = (warp >> 2) * 8 * WT, c0 = (warp & 3) * 8 * WT;
+  double acc[WT][WT][2];
+#pragma unroll
+  for (int i = 0; i < WT; ++i)
+#pragma unroll
+    for (int j = 0; j < WT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 16; k += 4) {
+    double af[WT], bf[WT];
+#pragma unroll
+    for (int i = 0; i < WT; ++i) af[i] = X[(r0 + 8 * i + g) * ldx + k + t];
+#pragma unroll
+    for (int j = 0; j < WT; ++j) bf[j] = U[(k + t) * ldu + c0 + 8 * j + g];
+#pragma unroll
+    for (int i = 0; i < WT; ++i)
+#pragma unroll
+      for (int j = 0; j < WT; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+  }
+#pragma unroll
+  for (int i = 0; i < WT; ++i)
+#pragma unroll
+    for (int j = 0; j < WT; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) fn(r0 + 8 * i + g, c0 + 8 * j + 2 * t + e, acc[i][j][e]);
+}
+
 // Inverse of a symmetric positive definite matrix held in shared memory,
 // in place, by block Gauss-Jordan sweeps over 16 x 16 pivot blocks:
 //   Dinv = K_PP^-1,  U = Dinv K_PQ,  W = K_QP Dinv,
@@ -424,19 +490,31 @@ __device__ __forceinline__ bool spd_inverse_blocked(double* K, int mp, int ld, d
     }
     __syncthreads();
     if (*flag == 0) return false;
-    // (2) U = Dinv K_P,:, W = K_:,P Dinv, and a copy X = K_:,P (old) for the update
+    // (2) U = Dinv K_P,:, W = K_:,P Dinv (their 16 x 16 blocks spread over all warps in one
+    // pass), and a copy X = K_:,P (old) for the update
     const double* Dinv = K + k0 * ld + k0;
-    smem_product<false, false>(b, mp, b, Dinv, ld, K + k0 * ld, ld,
-                               [&](int p, int j, double v) { U[p * ld + j] = v; });
-    smem_product<false, false>(mp, b, b, K + k0, ld, Dinv, ld,
-                               [&](int j, int p, double v) { W[j * 20 + p] = v; });
+    {
+      const int nb = mp / 16, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+      for (int blk = warp; blk < 2 * nb; blk += nwarps) {
+        if (blk < nb)
+          smem_block16<false, false>(0, blk * 16, Dinv, ld, K + k0 * ld, ld,
+                                     [&](int p, int j, double v) { U[p * ld + j] = v; });
+        else
+          smem_block16<false, false>((blk - nb) * 16, 0, K + k0, ld, Dinv, ld,
+                                     [&](int j, int p, double v) { W[j * 20 + p] = v; });
+      }
+    }
     for (int j = threadIdx.x >> 4; j < mp; j += blockDim.x >> 4) X[j * 20 + (threadIdx.x & 15)] = K[j * ld + k0 + (threadIdx.x & 15)];
     __syncthreads();
     // (3) K_QQ -= X U, K_PQ = U, K_QP = -W  (disjoint entries, one phase)
-    smem_product<false, false>(mp, mp, b, X, 20, U, ld, [&](int i, int j, double v) {
+    auto update = [&](int i, int j, double v) {
       const bool ip = i >= k0 && i < k0 + b, jp = j >= k0 && j < k0 + b;
       if (!ip && !jp) K[i * ld + j] -= v;
-    });
+    };
+    if (blockDim.x == kThreads && mp == 96) smem_rank16_tiled<3>(X, 20, U, ld, update);
+    else if (blockDim.x == kThreads && mp == 128) smem_rank16_tiled<4>(X, 20, U, ld, update);
+    else if (blockDim.x == kThreads && mp == 64) smem_rank16_tiled<2>(X, 20, U, ld, update);
+    else smem_product<false, false>(mp, mp, b, X, 20, U, ld, update);
     for (int p = threadIdx.x >> 5; p < b; p += blockDim.x >> 5)
       for (int j = threadIdx.x & 31; j < mp; j += 32) {
         if (j >= k0 && j < k0 + b) continue;
