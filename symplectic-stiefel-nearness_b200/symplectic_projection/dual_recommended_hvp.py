@@ -182,7 +182,28 @@ def solve(T: torch.Tensor, **options):
 
 # ---- host-resident batches: chunked, stream-pipelined staging ------------------------------
 CHUNK_BYTES = 64 * 2**20      # largest chunk of T, in bytes
-N_STREAMS = 8                 # chunks in flight; each solve is latency-bound, so they overlap
+N_STREAMS = 16                # chunks in flight; each solve is latency-bound, so they overlap
+CHUNK_RAMP = (1, 2, 4, 8)     # leading (and mirrored trailing) chunk sizes, in targets
+
+
+def _chunk_plan(batch: int, cap: int, ramp=None):
+    """Chunk sizes (targets) for the host pipeline.
+
+    A chunk's solve costs about one Newton latency whatever its size, and the two
+    copy directions run on separate engines.  Short chunks first let the copies
+    back start while later targets are still going up; short chunks last shorten
+    the tail (the last chunk's latency and its copy back).  Between the ramps the
+    chunks are as even as possible and at most ``cap`` targets.
+    """
+    ramp = tuple(CHUNK_RAMP if ramp is None else ramp)
+    if not ramp or batch < 2 * sum(ramp) + 1:
+        n = -(-batch // cap)
+        return [batch // n + (1 if i < batch % n else 0) for i in range(n)]
+    middle = batch - 2 * sum(ramp)
+    n = -(-middle // cap)
+    mid = [middle // n + (1 if i < middle % n else 0) for i in range(n)]
+    return list(ramp) + mid + list(reversed(ramp))
+
 
 _streams = {}
 _staging = {}
@@ -220,15 +241,17 @@ def _solve_host(T: torch.Tensor, **options):
     dev = torch.device("cuda", torch.cuda.current_device())
     X = _pinned_like(T)
     per = max(1, T[0].numel() * 8)
-    chunk = max(1, min(batch, CHUNK_BYTES // per, -(-batch // N_STREAMS)))
+    cap = max(1, min(batch, CHUNK_BYTES // per, -(-batch // N_STREAMS)))
+    sizes = _chunk_plan(batch, cap)
     pinned_in, pinned_out = T.is_pinned(), X.is_pinned()
     streams = _stream_pool(dev)
     main = torch.cuda.current_stream(dev)
     ready = torch.cuda.Event()
     ready.record(main)
     results, done = [], []
-    for idx, c0 in enumerate(range(0, batch, chunk)):
-        c1 = min(batch, c0 + chunk)
+    c1 = 0
+    for idx, size in enumerate(sizes):
+        c0, c1 = c1, c1 + size
         slot = idx % len(streams)
         s = streams[slot]
         s.wait_event(ready)

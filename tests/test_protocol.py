@@ -113,3 +113,14 @@ def test_ragged_workload_rule():
     assert [tuple(x.shape) for x in t] == [(128, 8), (64, 4), (128, 8)] and not torch.equal(t[0], t[2])
     g = torch.Generator().manual_seed(2026102300 + 1 + 2)
     assert torch.equal(t[2], torch.randn(128, 8, dtype=torch.float64, generator=g) / math.sqrt(128))
+
+
+def test_host_chunk_plan():
+    from symplectic_projection.dual_recommended_hvp import _chunk_plan
+    for batch in (1, 3, 7, 15, 16, 30, 31, 64, 100):
+        for cap in (1, 4, 8):
+            for ramp in ((), (1, 2, 4, 8), (2, 4)):
+                sizes = _chunk_plan(batch, cap, ramp)
+                assert sum(sizes) == batch and min(sizes) >= 1
+    assert _chunk_plan(64, 4, (1, 2, 4, 8)) == [1, 2, 4, 8] + [4] * 7 + [3, 3] + [8, 4, 2, 1]
+    assert _chunk_plan(10, 4, (1, 2, 4, 8)) == [4, 3, 3]               # too short for the ramps
