@@ -131,6 +131,16 @@ struct Dual {
     ssn::tile_product_staged<TL::WR, TL::WC, NA, NB, NOUT, COEF, dual_stages(MB, CL)>(
         As, B, rows, m, m, smem, dual_slot_a(MB, CL), dual_slot_b(MB), shifted);
   }
+
+  // All m rows by this CTA alone, in 32-row passes so that the A panels fit the A
+  // slots (sized for this CTA's own rows, >= 32 for every bucket a cluster runs).
+  // Each output entry sees the same DMMA sequence as in mul, so the same bits.
+  template <int NA, int NB, int NOUT, uint32_t COEF, class Epi>
+  __device__ __forceinline__ void mul_all(const MatOp (&A)[NA], const MatOp (&B)[NB], Epi& epi) const {
+    static_assert(CL == 1 || MB >= 2, "A slots hold at least 32 rows");
+    ssn::tile_product_staged<1, MB, NA, NB, NOUT, COEF, dual_stages(MB, CL)>(
+        A, B, m, m, m, smem, dual_slot_a(MB, CL), dual_slot_b(MB), epi);
+  }
 };
 
 // Element loops over this CTA's rows without integer division: warp w owns rows
@@ -195,6 +205,8 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   double* sdg = pdg + kMaxM;                  // kMaxM doubles: diag(Sr)
   double* xch = sdg + kMaxM;                  // 8 doubles
   int* flag = reinterpret_cast<int*>(xch + 8);
+  int* vflag = flag + 1;                      // cluster: the trial inverse's outcome, written by CTA 0
+  int* vflag_peer = vflag;
   double* Zs = smem;                          // this CTA's rows of the HVP outer product
   const int zld = m + 1;
 
@@ -212,6 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   if constexpr (CL == 2) {
     team.xch_peer = cg::this_cluster().map_shared_rank(xch, rank ^ 1);
     Zpeer = cg::this_cluster().map_shared_rank(Zs, rank ^ 1);
+    vflag_peer = cg::this_cluster().map_shared_rank(vflag, rank ^ 1);
     peer_r0 = imin(m, (rank ^ 1) * half);
   }
   Dual<MB, CL> eng{m, smem, team.r0, team.r1 - team.r0};
@@ -560,70 +573,133 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
         double* Ks = smem;
         const int mp16 = round_up(m, 16), kld = frag_ld(mp16);
         if constexpr (CL == 1) {
-          MatOp A[1] = {op_n(Wt, m)};
-          MatOp B[1] = {op_n(Wt, m)};
-          auto epi = [&](int, int i, int j, double v) {
-            Ks[i * kld + j] = __dadd_rn(i == j ? 1.0 : 0.0, v);
-          };
-          eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
-        } else {
-          // each CTA forms its rows of K in L2; both then invert the full K
-          MatOp A[1] = {op_n(Wt, m)};
-          MatOp B[1] = {op_n(Wt, m)};
-          auto epi = [&](int, int i, int j, double v) { Kg[i * m + j] = __dadd_rn(i == j ? 1.0 : 0.0, v); };
-          eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
-          team.sync();
-          for (int i = (int)(threadIdx.x >> 5); i < m; i += kWarps)
-            for (int j = (int)(threadIdx.x & 31); j < m; j += 32) Ks[i * kld + j] = Kg[i * m + j];
-        }
-        for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {   // identity padding up to mp16
-          const int i = e / mp16, j = e - i * mp16;
-          if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
-        }
-        __syncthreads();
-        const bool valid = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
-        if (valid) {
-          SSN_FOR_IJ(team, m, { Pt[e] = Ks[i * kld + j]; })
-        }
-        team.sync();
-        if (valid) {
-          // V = P_trial delta; dSr = delta Sr, dSi = delta Si (:177-178)
-          {
-            MatOp A[1] = {op_n(Pt, m)};
-            MatOp B[1] = {op_n(Dl, m)};
-            auto epi = store_to(T1);
-            eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
-          }
-          __syncthreads();
-          {
-            MatOp A[1] = {op_n(Dl, m)};
-            MatOp B[2] = {op_n(Sr, m), op_n(SiCur, m)};
-            auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T2 : T3)[i * m + j] = v; };
-            eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
-          }
-          team.sync();
-          // tail = <V, dSr + trial dSi> (line_change, hvp_fused.cu:259-371)
-          double tail = 0.0;
           {
             MatOp A[1] = {op_n(Wt, m)};
-            MatOp B[1] = {op_n(T3, m)};
+            MatOp B[1] = {op_n(Wt, m)};
             auto epi = [&](int, int i, int j, double v) {
-              const int e = i * m + j;
-              tail += __dmul_rn(T1[e], __dadd_rn(T2[e], v));
+              Ks[i * kld + j] = __dadd_rn(i == j ? 1.0 : 0.0, v);
             };
             eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
           }
-          tail = team.sum(tail);
-          const double change = __dadd_rn(first, tail);
-          if (change <= 1e-4 * t * slope) {
-            double* tmp = Wm;
-            Wm = Wt;
-            Wt = tmp;
-            tmp = Pm;
-            Pm = Pt;
-            Pt = tmp;
-            accepted = true;
-            break;
+          for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {   // identity padding up to mp16
+            const int i = e / mp16, j = e - i * mp16;
+            if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
+          }
+          __syncthreads();
+          const bool valid = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
+          if (valid) {
+            SSN_FOR_IJ(team, m, { Pt[e] = Ks[i * kld + j]; })
+          }
+          __syncthreads();
+          if (valid) {
+            // V = P_trial delta; dSr = delta Sr, dSi = delta Si (:177-178)
+            {
+              MatOp A[1] = {op_n(Pt, m)};
+              MatOp B[1] = {op_n(Dl, m)};
+              auto epi = store_to(T1);
+              eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+            }
+            __syncthreads();
+            {
+              MatOp A[1] = {op_n(Dl, m)};
+              MatOp B[2] = {op_n(Sr, m), op_n(SiCur, m)};
+              auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T2 : T3)[i * m + j] = v; };
+              eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
+            }
+            __syncthreads();
+            // tail = <V, dSr + trial dSi> (line_change, hvp_fused.cu:259-371)
+            double tail = 0.0;
+            {
+              MatOp A[1] = {op_n(Wt, m)};
+              MatOp B[1] = {op_n(T3, m)};
+              auto epi = [&](int, int i, int j, double v) {
+                const int e = i * m + j;
+                tail += __dmul_rn(T1[e], __dadd_rn(T2[e], v));
+              };
+              eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+            }
+            tail = team.sum(tail);
+            const double change = __dadd_rn(first, tail);
+            if (change <= 1e-4 * t * slope) {
+              double* tmp = Wm;
+              Wm = Wt;
+              Wt = tmp;
+              tmp = Pm;
+              Pm = Pt;
+              Pt = tmp;
+              accepted = true;
+              break;
+            }
+          }
+        } else {
+          // Cluster: each CTA forms its rows of K in L2.  Then CTA 0 alone inverts K
+          // while CTA 1 forms, for all rows, the trial's products that do not need the
+          // inverse: U = delta Sr + trial (delta Si) (line_change's dSr + trial dSi).
+          // Every cluster barrier below is reached by both CTAs on every trial.
+          {
+            MatOp A[1] = {op_n(Wt, m)};
+            MatOp B[1] = {op_n(Wt, m)};
+            auto epi = [&](int, int i, int j, double v) { Kg[i * m + j] = __dadd_rn(i == j ? 1.0 : 0.0, v); };
+            eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+          }
+          team.sync();
+          if (rank == 0) {
+            for (int i = (int)(threadIdx.x >> 5); i < m; i += kWarps)
+              for (int j = (int)(threadIdx.x & 31); j < m; j += 32) Ks[i * kld + j] = Kg[i * m + j];
+            for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {   // identity padding up to mp16
+              const int i = e / mp16, j = e - i * mp16;
+              if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
+            }
+            __syncthreads();
+            const bool ok = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
+            if (threadIdx.x == 0) {
+              vflag[0] = ok ? 1 : 0;
+              vflag_peer[0] = ok ? 1 : 0;
+            }
+            if (ok)
+              for (int i = (int)(threadIdx.x >> 5); i < m; i += kWarps)
+                for (int j = (int)(threadIdx.x & 31); j < m; j += 32) Pt[i * m + j] = Ks[i * kld + j];
+          } else {
+            {
+              MatOp A[1] = {op_n(Dl, m)};
+              MatOp B[2] = {op_n(Sr, m), op_n(SiCur, m)};
+              auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T2 : T3)[i * m + j] = v; };
+              eng.template mul_all<1, 2, 2, C_SHARED_A>(A, B, epi);
+            }
+            __syncthreads();
+            {
+              MatOp A[1] = {op_n(Wt, m)};
+              MatOp B[1] = {op_n(T3, m)};
+              auto epi = [&](int, int i, int j, double v) {
+                const int e = i * m + j;
+                T2[e] = __dadd_rn(T2[e], v);
+              };
+              eng.template mul_all<1, 1, 1, C_ONE>(A, B, epi);
+            }
+          }
+          team.sync();
+          const bool valid = *reinterpret_cast<volatile int*>(vflag) != 0;
+          if (valid) {
+            // tail = <P_trial delta, U> over this CTA's rows (line_change, hvp_fused.cu:259-371)
+            double tail = 0.0;
+            {
+              MatOp A[1] = {op_n(Pt, m)};
+              MatOp B[1] = {op_n(Dl, m)};
+              auto epi = [&](int, int i, int j, double v) { tail += __dmul_rn(v, T2[i * m + j]); };
+              eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+            }
+            tail = team.sum(tail);
+            const double change = __dadd_rn(first, tail);
+            if (change <= 1e-4 * t * slope) {
+              double* tmp = Wm;
+              Wm = Wt;
+              Wt = tmp;
+              tmp = Pm;
+              Pm = Pt;
+              Pt = tmp;
+              accepted = true;
+              break;
+            }
           }
         }
         t = t / 2;
