@@ -207,6 +207,7 @@ def run_ours(args):
     import symplectic_projection as sp
     from symplectic_projection import _native as N
     from symplectic_projection.certify import certify
+    from symplectic_projection.replicas import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -304,10 +305,7 @@ def run_ours(args):
             dist.barrier()
         clocks = sampler.stop()
         total_ms = start.elapsed_time(end)
-        if world > 1:
-            t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t[0])
+        total_ms = max_over_ranks(total_ms, dev)
 
         # correctness of the timed outputs: every instance converged and passes the checks
         st = status.cpu()
@@ -411,10 +409,7 @@ def run_ours(args):
         if i > 1:
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_step = sum(e2e_ms) / max(1, len(e2e_ms))
-    if world > 1:
-        t = torch.tensor([e2e_step], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_step = float(t[0])
+    e2e_step = max_over_ranks(e2e_step, dev)
     h2d = T_host.numel() * 8
     d2h = X_host.numel() * 8 + W_host.numel() * 8 + I_host.numel() * 8 + B * 4
     # raw pinned copy rates of this host link (the floor of the end-to-end number)
