@@ -38,9 +38,9 @@ PRECISION_NOTE = {
 }
 N_DEFAULT, K_DEFAULT, BATCH_DEFAULT = 4096, 48, 64
 # DRAM bytes (read + write) of the Newton kernel per target at n = 4096, k = 48, from one ncu
-# capture of 24 targets (dram__bytes_read.sum + dram__bytes_write.sum = 5.866 MB + 2.218 MB);
+# capture of 24 targets (dram__bytes_read.sum + dram__bytes_write.sum = 5.852 MB + 2.077 MB);
 # each target's state is private, so traffic scales with the number of targets.
-NEWTON_DRAM_BYTES_PER_TARGET_C2 = (5866240 + 2217728) / 24
+NEWTON_DRAM_BYTES_PER_TARGET_C2 = (5851648 + 2076928) / 24
 HBM_FALLBACK_GBS = 6650.0        # copy bandwidth of this GPU type when no measured figure is present
 
 
