@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
                          double* __restrict__ scale_out, int32_t* __restrict__ sweeps_out,
                          int32_t* __restrict__ status_out, Real* __restrict__ rlog,
                          int32_t* __restrict__ nsteps_out, int32_t* __restrict__ order_out, int m,
-                         int max_sweeps, int strict) {
+                         int max_sweeps, int strict, float skip_corr) {
   using V2 = typename JReal<Real>::V2;
   extern __shared__ __align__(16) double sm_raw[];
   Real* sm = reinterpret_cast<Real*>(sm_raw);
@@ -129,6 +129,32 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   for (int e = tid; e < m * m; e += kJacobiThreads) {
     const int i = e / m, j = e - i * m;
     A[i * ld + j] = static_cast<Real>(C[e] / scale);
+  }
+  // rough basis (skip_corr > 0): when every off-diagonal correlation
+  // |a_pq| / sqrt(a_pp a_qq) of the scaled Gram is below skip_corr, the identity
+  // already nearly diagonalises it and no sweep is run (a CTA-wide max, so every
+  // thread takes the same decision)
+  int sweeps_cap = max_sweeps;
+  if (skip_corr > 0.0f) {
+    double mx = 0.0;
+    for (int e = tid; e < m * m; e += kJacobiThreads) {
+      const int i = e / m, j = e - i * m;
+      if (i < j) {
+        const double d = C[(size_t)i * m + i] * C[(size_t)j * m + j];
+        const double c = fabs(C[e]);
+        if (d > 0.0) mx = fmax(mx, c / sqrt(d));
+        else if (c > 0.0 || !(d == 0.0)) mx = fmax(mx, 1.0);   // non-finite or inconsistent: keep the sweeps
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    __syncthreads();
+    if ((tid & 31) == 0) red[tid >> 5] = mx;
+    __syncthreads();
+    double all = 0.0;
+    for (int w = 0; w < kJacobiThreads / 32; ++w) all = fmax(all, red[w]);
+    if (!(all >= static_cast<double>(skip_corr))) sweeps_cap = 0;
+    __syncthreads();
   }
   // block list: off-diagonal blocks (a < b) row-major, then the diagonal blocks.
   // Host blocks carry kHostFlag in .y and are skipped by the generic threads.
@@ -180,7 +206,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
 
   int g = 0, st = 0, sweep = 0;
   bool converged = false;
-  const int max_steps = imin(max_sweeps, kMaxSweeps) * m1;
+  const int max_steps = imin(sweeps_cap, kMaxSweeps) * m1;
   while (g < max_steps) {
     const int cur = g & 1, nxt = cur ^ 1;
     const int nsweep = (st + 1 == m1) ? sweep + 1 : sweep;
@@ -393,7 +419,7 @@ size_t eigh_workspace_bytes(int batch, int m) {
 template <class Real>
 static cudaError_t launch_eigh_t(const double* Cr, double* values, double* vectors, double* scale,
                                  int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
-                                 int max_sweeps, bool strict, cudaStream_t stream) {
+                                 int max_sweeps, bool strict, float skip_corr, cudaStream_t stream) {
   Real* rlog = static_cast<Real*>(workspace);
   int32_t* nsteps = reinterpret_cast<int32_t*>(static_cast<double*>(workspace) + eigh_log_doubles(batch, m));
   int32_t* order = nsteps + batch;
@@ -402,7 +428,8 @@ static cudaError_t launch_eigh_t(const double* Cr, double* values, double* vecto
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;
   jacobi_values_kernel<Real><<<batch, kJacobiThreads, smem, stream>>>(Cr, values, scale, sweeps, status, rlog,
-                                                                     nsteps, order, m, max_sweeps, strict ? 1 : 0);
+                                                                     nsteps, order, m, max_sweeps, strict ? 1 : 0,
+                                                                     skip_corr);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   const size_t vsmem = sizeof(Real) * (2 * kVecChunk * (m / 2) + kVecWarps * (m + 1)) +
@@ -419,18 +446,18 @@ cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, doubl
                         int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
                         cudaStream_t stream) {
   return launch_eigh_t<double>(Cr, values, vectors, scale, sweeps, status, batch, m, workspace, kMaxSweeps,
-                               true, stream);
+                               true, 0.0f, stream);
 }
 
 cudaError_t launch_eigh_approx(const double* Cr, double* values, double* vectors, double* scale,
                                int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
-                               int max_sweeps, bool fp32, cudaStream_t stream) {
+                               int max_sweeps, bool fp32, float skip_corr, cudaStream_t stream) {
   if (max_sweeps < 1) max_sweeps = 1;
   if (max_sweeps > kMaxSweeps) max_sweeps = kMaxSweeps;
   return fp32 ? launch_eigh_t<float>(Cr, values, vectors, scale, sweeps, status, batch, m, workspace,
-                                     max_sweeps, false, stream)
+                                     max_sweeps, false, skip_corr, stream)
               : launch_eigh_t<double>(Cr, values, vectors, scale, sweeps, status, batch, m, workspace,
-                                      max_sweeps, false, stream);
+                                      max_sweeps, false, skip_corr, stream);
 }
 
 }  // namespace ssn

@@ -81,10 +81,12 @@ cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, doubl
                         int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
                         cudaStream_t stream);
 // Jacobi capped at max_sweeps (no convergence requirement), FP32 or FP64 rotations:
-// the rough eigenbasis of the split-precision form.
+// the rough eigenbasis of the split-precision form.  skip_corr > 0: an instance whose
+// largest off-diagonal correlation |c_pq| / sqrt(c_pp c_qq) is below skip_corr gets no
+// sweep (identity basis).
 cudaError_t launch_eigh_approx(const double* Cr, double* values, double* vectors, double* scale,
                                int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
-                               int max_sweeps, bool fp32, cudaStream_t stream);
+                               int max_sweeps, bool fp32, float skip_corr, cudaStream_t stream);
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
 // The whole uniform-batch solve (the body of ssn_solve) on one stream; `concurrent` as in DualArgs.
 int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch,
