@@ -24,7 +24,7 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Workspace layout of ssn_solve (byte offsets, 256-byte aligned sections).
 struct SolveLayout {
-  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, eig_ws, rec, stall, total;
+  size_t cr, ci, values, vectors, scale, pfin, qfin, work, eig_status, sweeps, eig_ws, rec, stall, total;
 };
 
 SolveLayout solve_layout(int batch, int n, int m) {
@@ -50,6 +50,7 @@ SolveLayout solve_layout(int batch, int n, int m) {
   if (oz > partial) partial = oz;
   L.work = take(work > partial ? work : partial);
   L.eig_status = take(sizeof(int32_t) * batch);
+  L.sweeps = take(sizeof(int32_t) * batch);
   L.eig_ws = take(eigh_workspace_bytes(batch, m));
   // split form: the recovery's digits of [A | D] (made early, alongside the Newton phase)
   L.rec = take(ozaki_recover_workspace_bytes(batch, n, m));
@@ -208,7 +209,8 @@ int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, 
     if (e == cudaSuccess) e = side.record();
     if (e != cudaSuccess) return SSN_ERR_CUDA;
   }
-  e = eigenbasis(opt, Cr, values, vectors, scale, nullptr, eig_status, batch, m, ws + L.eig_ws, stream);
+  int32_t* sweeps = reinterpret_cast<int32_t*>(ws + L.sweeps);
+  e = eigenbasis(opt, Cr, values, vectors, scale, sweeps, eig_status, batch, m, ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   DualArgs a{};
   a.m = m;
@@ -219,6 +221,7 @@ int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, 
   a.vectors = vectors;
   a.scale = scale;
   a.eig_status = eig_status;
+  a.sweeps = sweeps;
   a.work = work;
   a.omega = omega;
   a.P = Pf;

@@ -273,7 +273,8 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
     // ---- eigenbasis set-up: Ce = skew(V^T (Ci/s) V), Je = skew(V^T J(V)) / s  (:106-111, :53-56)
     const int h = m / 2;
     double* CrE = ws + (size_t)M_X2 * mm;       // approximate basis: sym(V^T (Cr/s) V)
-    if (a.approx_basis && a.orthogonalize) {
+    // (the same bits for both CTAs of a cluster, so both take the same branch and barriers)
+    if (a.approx_basis && a.orthogonalize && !(a.sweeps && a.sweeps[inst] == 0)) {
       // V <- V (3I - V^T V) / 2 twice: vectors from FP32 rotations become orthogonal to FP64 rounding
       double* Vb[2] = {ws + (size_t)M_X2 * mm, ws + (size_t)M_X1 * mm};
       const double* Vin = V;

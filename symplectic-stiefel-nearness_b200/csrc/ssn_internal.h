@@ -22,6 +22,8 @@ struct DualArgs {
   const double* vectors;   // [B,m,m] eigenvectors
   const double* scale;     // [B]
   const int32_t* eig_status;  // [B]
+  const int32_t* sweeps;      // [B] Jacobi sweeps of the basis, or null: 0 means the identity
+                              // basis (a permutation), which needs no re-orthogonalisation
   double* work;            // [B, kDualMats, m, m]
   double* omega;           // [B,m,m] out, original basis
   double* P;               // [B,m,m] out
