@@ -73,7 +73,9 @@ typedef struct {
   int max_backtrack; /* 40  */
   double feas_tol;   /* 1e-8: an instance is done when residual < feas_tol / 2 */
   int precision;     /* SSN_PRECISION_FP64 (default) or SSN_PRECISION_SPLIT */
-  int eig_sweeps;    /* split form: Jacobi sweeps of the rough eigenbasis (0 = default 1, max 24) */
+  int eig_sweeps;    /* split form: Jacobi sweeps of the rough eigenbasis (max 24); 0 = default:
+                        no sweep when every off-diagonal correlation of the scaled Gram is
+                        below 0.1 (identity basis), else 1 */
   int preconditioner; /* SSN_PRECOND_EIGENBASIS (default) or SSN_PRECOND_ADAPTIVE */
   int reserved[5];
 } ssn_options;
