@@ -122,8 +122,14 @@ def solve_ragged(targets, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
         ns.append(rows // 2)
         ms.append(m)
     dev = torch.device("cuda", torch.cuda.current_device()) if on_host else targets[0].device
-    flat = torch.cat([t.reshape(-1) for t in targets])
-    flat = flat.to(dev, non_blocking=False) if on_host else flat
+    if on_host:
+        # one pinned staging buffer: the copy up runs at the link's pinned rate
+        total = sum(t.numel() for t in targets)
+        staged = torch.empty(total, dtype=torch.float64, pin_memory=True)
+        torch.cat([t.reshape(-1) for t in targets], out=staged)
+        flat = staged.to(dev, non_blocking=True)
+    else:
+        flat = torch.cat([t.reshape(-1) for t in targets])
     count = len(targets)
     t_off = [0] * count
     w_off = [0] * count
@@ -149,7 +155,10 @@ def solve_ragged(targets, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
     if raise_on_failure:
         raise_for_status(status)
     if on_host:
-        X, omega, iterations, status = X.cpu(), omega.cpu(), iterations.cpu(), status.cpu()
+        X_host = torch.empty(X.shape, dtype=X.dtype, pin_memory=True)
+        X_host.copy_(X, non_blocking=True)
+        omega, iterations, status = omega.cpu(), iterations.cpu(), status.cpu()   # synchronises
+        X = X_host
     Xs = [X[t_off[i]:t_off[i] + 2 * ns[i] * ms[i]].view(2 * ns[i], ms[i]) for i in range(count)]
     Ws = [omega[w_off[i]:w_off[i] + ms[i] * ms[i]].view(ms[i], ms[i]) for i in range(count)]
     return Xs, Ws, iterations, status
