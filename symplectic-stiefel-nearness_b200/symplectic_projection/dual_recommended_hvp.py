@@ -193,6 +193,8 @@ def solve(T: torch.Tensor, **options):
 CHUNK_BYTES = 64 * 2**20      # largest chunk of T, in bytes
 N_STREAMS = 16                # chunks in flight; each solve is latency-bound, so they overlap
 CHUNK_RAMP = (1, 2, 4, 8)     # leading (and mirrored trailing) chunk sizes, in targets
+MIN_CHUNK_BYTES = 16 * 2**20  # smallest chunk between the ramps: per-chunk launch work stays small
+RAMP_MIN_BYTES = 256 * 2**20  # ramps only for batches this large, where the copies dominate
 
 
 def _chunk_plan(batch: int, cap: int, ramp=None):
@@ -250,8 +252,8 @@ def _solve_host(T: torch.Tensor, **options):
     dev = torch.device("cuda", torch.cuda.current_device())
     X = _pinned_like(T)
     per = max(1, T[0].numel() * 8)
-    cap = max(1, min(batch, CHUNK_BYTES // per, -(-batch // N_STREAMS)))
-    sizes = _chunk_plan(batch, cap)
+    cap = max(1, min(batch, CHUNK_BYTES // per, max(-(-batch // N_STREAMS), MIN_CHUNK_BYTES // per)))
+    sizes = _chunk_plan(batch, cap, None if batch * per >= RAMP_MIN_BYTES else ())
     pinned_in, pinned_out = T.is_pinned(), X.is_pinned()
     streams = _stream_pool(dev)
     main = torch.cuda.current_stream(dev)
