@@ -11,6 +11,7 @@ batch on a Newton or line-search cap, as the reference does
 """
 from __future__ import annotations
 
+import threading
 from dataclasses import dataclass
 
 import torch
@@ -218,6 +219,9 @@ def _chunk_plan(batch: int, cap: int, ramp=None):
 
 _streams = {}
 _staging = {}
+# The stream pool and the pinned staging buffers are shared per device, so host-path
+# solves from several Python threads take turns (device-resident solves do not lock).
+_host_lock = threading.Lock()
 
 
 def _stream_pool(dev: torch.device):
@@ -240,6 +244,11 @@ def _staging_buffer(dev: torch.device, slot: int, shape) -> torch.Tensor:
 
 
 def _solve_host(T: torch.Tensor, **options):
+    with _host_lock:
+        return _solve_host_locked(T, **options)
+
+
+def _solve_host_locked(T: torch.Tensor, **options):
     """CPU-in/CPU-out solve with the batch split into chunks on a pool of streams.
 
     Each chunk's H2D copy, solve and D2H copy are enqueued on one stream, so
