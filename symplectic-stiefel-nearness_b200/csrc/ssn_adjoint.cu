@@ -23,7 +23,7 @@ namespace {
 size_t align_up_256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct AdjointLayout {
-  size_t partial, cr, ci, mr, mi, p, q, pn, qn, work, tmp, total;
+  size_t partial, cr, ci, mr, mi, p, q, pn, qn, work, tmp, oz, stall, total;
 };
 
 AdjointLayout adjoint_layout(int batch, int n, int m) {
@@ -46,6 +46,10 @@ AdjointLayout adjoint_layout(int batch, int n, int m) {
   L.qn = take(sizeof(double) * batch * mm);
   L.work = take(sizeof(double) * (size_t)batch * kAdjointMats * mm);
   L.tmp = take(sizeof(double) * (size_t)batch * 2 * n * m);
+  // split form: the INT8 Ozaki Gram and recoveries (used one after the other)
+  const size_t og = ozaki_gram_workspace_bytes(batch, n, m), orc = ozaki_recover_workspace_bytes(batch, n, m);
+  L.oz = take(og > orc ? og : orc);
+  L.stall = take(sizeof(int32_t) * 4);
   L.total = off;
   return L;
 }
@@ -96,7 +100,20 @@ int ssn_adjoint(const double* T, const double* omega, const double* G, const dou
   const int64_t stride = 2LL * n * m;
   const size_t mm = (size_t)m * m;
 
-  cudaError_t e = launch_gram(T, T + (size_t)n * m, stride, Cr, Ci, batch, n, m, partial, stream);
+  // opt->precision == SSN_PRECISION_SPLIT: the Gram of T and the two recoveries run as INT8
+  // Ozaki products on the tensor cores (the cross Gram stays FP64)
+  const bool split = opt && opt->precision == SSN_PRECISION_SPLIT;
+  void* oz = ws + L.oz;
+  int* stall = reinterpret_cast<int*>(ws + L.stall);
+  auto recover = [&](const double* A, const double* P, const double* Q, double* U) {
+    return split ? launch_recover_ozaki(A, A + (size_t)n * m, stride, P, Q, U, U + (size_t)n * m, stride, batch, n,
+                                        m, oz, stream)
+                 : launch_recover(A, A + (size_t)n * m, stride, P, Q, U, U + (size_t)n * m, stride, batch, n, m,
+                                  stream);
+  };
+  cudaError_t e = split ? launch_gram_ozaki(T, T + (size_t)n * m, stride, Cr, Ci, batch, n, m, oz, nullptr, stall,
+                                            stream)
+                        : launch_gram(T, T + (size_t)n * m, stride, Cr, Ci, batch, n, m, partial, stream);
   if (e == cudaSuccess) {
     if (G)
       e = launch_cross_gram(G, G + (size_t)n * m, stride, T, T + (size_t)n * m, stride, Mr, Mi, batch, n, m,
@@ -128,21 +145,17 @@ int ssn_adjoint(const double* T, const double* omega, const double* G, const dou
   e = launch_adjoint(a, batch, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
 
-  double* top = dT;
-  double* bot = dT + (size_t)n * m;
   if (G) {
     double* tmp = reinterpret_cast<double*>(ws + L.tmp);
-    e = launch_recover(G, G + (size_t)n * m, stride, a.P, a.Q, top, bot, stride, batch, n, m, stream);
-    if (e == cudaSuccess)
-      e = launch_recover(T, T + (size_t)n * m, stride, a.Pn, a.Qn, tmp, tmp + (size_t)n * m, stride, batch, n, m,
-                         stream);
+    e = recover(G, a.P, a.Q, dT);
+    if (e == cudaSuccess) e = recover(T, a.Pn, a.Qn, tmp);
     if (e == cudaSuccess) {
       const int64_t n2 = (int64_t)batch * stride / 2;
       add_into_kernel<<<4 * 148, 256, 0, stream>>>(dT, tmp, n2);
       e = cudaGetLastError();
     }
   } else {
-    e = launch_recover(T, T + (size_t)n * m, stride, a.Pn, a.Qn, top, bot, stride, batch, n, m, stream);
+    e = recover(T, a.Pn, a.Qn, dT);
   }
   return e == cudaSuccess ? SSN_OK : SSN_ERR_CUDA;
 }

@@ -21,11 +21,14 @@ _MESSAGES = {3: "adjoint CG reached its iteration cap", 5: "adjoint: non-finite 
 
 @torch.no_grad()
 def solve_backward(T: torch.Tensor, omega: torch.Tensor, grad_X: torch.Tensor | None = None,
-                   grad_omega: torch.Tensor | None = None, *, max_cg: int = 0, raise_on_failure: bool = True):
+                   grad_omega: torch.Tensor | None = None, *, precision: str = "fp64", max_cg: int = 0,
+                   raise_on_failure: bool = True):
     """(dL/dT, status, cg_iterations) for L with dL/dX = grad_X and dL/d omega = grad_omega.
 
     T [batch, 2n, 2k] and omega [batch, 2k, 2k] (the solve's multiplier) are CUDA
-    float64 tensors; either gradient may be None (treated as zero).
+    float64 tensors; either gradient may be None (treated as zero).  precision="split"
+    runs the Gram of T and the two recovery products as INT8 Ozaki products on the
+    tensor cores; the Hessian solve is FP64 in both forms.
     """
     batch, n, m = _check_target(T)
     dev = N.require_cuda_f64(T, omega)
@@ -46,7 +49,7 @@ def solve_backward(T: torch.Tensor, omega: torch.Tensor, grad_X: torch.Tensor | 
     lib = N.load()
     nbytes = lib.ssn_adjoint_workspace_bytes(batch, n, m)
     ws = workspace(dev, nbytes)
-    opt = N.options(max_cg=max(1, max_cg)) if max_cg else None
+    opt = N.options(max_cg=max(1, max_cg), precision=precision) if max_cg else N.options(precision=precision)
     N.check(lib.ssn_adjoint(T.data_ptr(), omega.data_ptr(), N.ptr(grad_X), N.ptr(grad_omega), dT.data_ptr(),
                             status.data_ptr(), iters.data_ptr(), batch, n, m, ws.data_ptr(), nbytes,
                             N.ctypes.byref(opt) if opt is not None else None, N.stream_handle(dev)), "ssn_adjoint")
@@ -66,12 +69,13 @@ class SymplecticProjection(torch.autograd.Function):
         res = solve_ex(T, **options)
         raise_for_status(res.status)
         ctx.save_for_backward(T, res.omega)
+        ctx.precision = options.get("precision", "fp64")
         return res.X, res.omega
 
     @staticmethod
     def backward(ctx, grad_X, grad_omega):
         T, omega = ctx.saved_tensors
-        dT, _, _ = solve_backward(T, omega, grad_X, grad_omega)
+        dT, _, _ = solve_backward(T, omega, grad_X, grad_omega, precision=ctx.precision)
         return dT, None
 
 
