@@ -127,3 +127,26 @@ def test_split_benchmark_config_parity(sp, n, k, case):
     assert int((I - Io).abs().max()) <= 1
     recs = O.inspect_output(T, X)
     assert all(O.passes(r) for r in recs), O.worst(recs)
+
+
+def test_split_default_basis_choice(sp):
+    """With the default sweep count the split form keeps the identity basis for nearly
+    diagonal Grams (Gaussian targets) and runs one sweep otherwise; explicit counts are kept."""
+    from symplectic_projection.dual_recommended_hvp import eigh_scaled
+    from symplectic_projection.inputs import illcond_targets
+    Tg, _ = O.make_inputs(4096, 48, 5, 3)                   # largest correlation ~ 4/sqrt(8192)
+    Ti = illcond_targets(512, 16, 2)
+    Crg, _ = O.gram(Tg)
+    Cri, _ = O.gram(Ti)
+    _, Vg, _, sw_g = eigh_scaled(Crg.cuda(), precision="split")
+    _, Vi, _, sw_i = eigh_scaled(Cri.cuda(), precision="split")
+    assert sw_g.cpu().tolist() == [0, 0, 0] and sw_i.cpu().tolist() == [1, 1]
+    Vg = Vg.cpu()
+    assert torch.equal(Vg.abs().sum(dim=1), torch.ones(3, 96, dtype=torch.float64))   # a permutation
+    _, _, _, sw_x = eigh_scaled(Crg.cuda(), precision="split", eig_sweeps=2)
+    assert sw_x.cpu().tolist() == [2, 2, 2]
+    # and the identity basis still solves to the oracle's X
+    res = sp.solve_ex(Tg.cuda(), precision="split")
+    Xo, Wo, _ = O.solve(Tg)
+    assert res.status.cpu().tolist() == [0, 0, 0]
+    assert rel_per_instance(res.X, Xo) < XTOL and rel_per_instance(res.omega, Wo) < XTOL
