@@ -826,24 +826,41 @@ cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
 enum AdjMat { A_SR = 0, A_SI, A_DN, A_MU, A_R, A_PP, A_T1, A_T2, A_Y1, A_Y2 };
 static_assert(A_Y2 + 1 <= kAdjointMats, "adjoint workspace matrix count");
 
-template <int MB>
+template <int MB, int CL>
 __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
   extern __shared__ __align__(16) double smem[];
-  const int m = a.m, mm = m * m, inst = blockIdx.x;
-  constexpr int region = dual_region_doubles(MB, 1);
+  const int m = a.m, mm = m * m;
+  const int rank = CL == 1 ? 0 : (int)cg::this_cluster().block_rank();
+  const int inst = blockIdx.x / CL;
+  constexpr int region = dual_region_doubles(MB, CL);
   double* red = smem + region;                // 2*kWarps doubles
-  int* flag = reinterpret_cast<int*>(red + 2 * kWarps);
-  double* Zs = smem;                          // rows of the HVP outer product
+  double* xch = red + 2 * kWarps;             // 8 doubles: cluster exchange slots
+  int* flag = reinterpret_cast<int*>(xch + 8);
+  double* pdg = xch + 16;                     // kMaxM doubles: diag(P)
+  double* sdg = pdg + kMaxM;                  // kMaxM doubles: diag(Sr)
+  double* Zs = smem;                          // this CTA's rows of the HVP outer product
   const int zld = m + 1;
-  Team<1> team;
-  team.rank = 0;
-  team.r0 = 0;
-  team.r1 = m;
+  const int half = round_up(cdiv(m, CL), 8);
+  Team<CL> team;
+  team.rank = rank;
+  team.r0 = imin(m, rank * half);
+  team.r1 = imin(m, (rank + 1) * half);
   team.red = red;
-  team.xch = red;
-  team.xch_peer = red;
+  team.xch = xch;
+  team.xch_peer = xch;
   team.parity = 0;
-  Dual<MB, 1> eng{m, smem, 0, m};
+  const double* Zpeer = Zs;
+  int peer_r0 = 0;
+  if constexpr (CL == 2) {
+    team.xch_peer = cg::this_cluster().map_shared_rank(xch, rank ^ 1);
+    Zpeer = cg::this_cluster().map_shared_rank(Zs, rank ^ 1);
+    peer_r0 = imin(m, (rank ^ 1) * half);
+  }
+  auto zval = [&](int j, int i) -> double {
+    if (CL == 1 || (j >= team.r0 && j < team.r1)) return Zs[(j - team.r0) * zld + i];
+    return Zpeer[(j - peer_r0) * zld + i];
+  };
+  Dual<MB, CL> eng{m, smem, team.r0, team.r1 - team.r0};
 
   double* ws = a.work + (size_t)inst * kAdjointMats * mm;
   double* Sr = ws + (size_t)A_SR * mm;
@@ -869,14 +886,24 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
   int status = SSN_INSTANCE_CONVERGED;
   int iters = 0;
 
-  // P = (I + omega omega)^-1 with the positive-definiteness test, Q = -omega P
+  // P = (I + omega omega)^-1 with the positive-definiteness test, Q = -omega P.  In a cluster
+  // each CTA forms its rows of K in L2 (Y1 as scratch) and both invert the full K, so both
+  // take the same decision.
   {
     double* Ks = smem;
     const int mp16 = round_up(m, 16), kld = frag_ld(mp16);
     MatOp A[1] = {op_n(W, m)};
     MatOp B[1] = {op_n(W, m)};
-    auto epi = [&](int, int i, int j, double v) { Ks[i * kld + j] = (i == j ? 1.0 : 0.0) + v; };
-    eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+    if constexpr (CL == 1) {
+      auto epi = [&](int, int i, int j, double v) { Ks[i * kld + j] = (i == j ? 1.0 : 0.0) + v; };
+      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+    } else {
+      auto epi = [&](int, int i, int j, double v) { Y1[i * m + j] = (i == j ? 1.0 : 0.0) + v; };
+      eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+      team.sync();
+      for (int i = (int)(threadIdx.x >> 5); i < m; i += kWarps)
+        for (int j = (int)(threadIdx.x & 31); j < m; j += 32) Ks[i * kld + j] = Y1[i * m + j];
+    }
     for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {
       const int i = e / mp16, j = e - i * mp16;
       if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
@@ -888,7 +915,7 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
     } else {
       status = SSN_INSTANCE_NONFINITE;
     }
-    __syncthreads();
+    team.sync();
   }
   if (status == SSN_INSTANCE_CONVERGED) {
     {
@@ -897,8 +924,8 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
       auto epi = [&](int, int i, int j, double v) { Qm[i * m + j] = -v; };
       eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
     }
-    __syncthreads();
-    // Y = K C, then S = Y K (Sr symmetric, Si antisymmetric parts)
+    team.sync();
+    // Y = K C (this CTA's rows), then S = Y K; symmetric / antisymmetric parts need all rows
     {
       MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
       MatOp B[2] = {op_n(Cr, m), op_n(Ci, m)};
@@ -912,7 +939,7 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
       auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T2)[i * m + j] = v; };
       eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
     }
-    __syncthreads();
+    team.sync();
     each_ij<MB>(team, m,
         [&](int i, int j, int e) {
           const int et = j * m + i;
@@ -922,8 +949,8 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
           Sr[e] = (v.x + v.y) / 2;
           Si[e] = (v.z - v.w) / 2;
         });
-    __syncthreads();
-    // Y = K M, then Im(Y K) = Y1 Q + Y2 P
+    team.sync();
+    // Y = K M, then Im(Y K) = Y1 Q + Y2 P (this CTA's rows)
     {
       MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
       MatOp B[2] = {op_n(Mr, m), op_n(Mi, m)};
@@ -937,37 +964,33 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
       auto epi = [&](int, int i, int j, double v) { T2[i * m + j] = v; };
       eng.template mul<2, 2, 1, C_SHARED_SUM>(A, B, epi);
     }
-    __syncthreads();
+    team.sync();
     // Gamma = -skew(Im(K M K)) + skew(G_omega) (exactly antisymmetric), preconditioner,
     // CG start: mu = 0, r = Gamma, p = r / den
     for (int i = threadIdx.x; i < m; i += kThreads) {
-      red[2 * kWarps + 16 + i] = Pm[i * m + i];
+      pdg[i] = Pm[i * m + i];
+      sdg[i] = Sr[i * m + i];
     }
+    __syncthreads();
     double gn2 = 0.0, rz = 0.0;
-    {
-      double* pdg = red + 2 * kWarps + 16;              // diag(P) then diag(Sr), staged in shared memory
-      double* sdg = pdg + kMaxM;
-      for (int i = threadIdx.x; i < m; i += kThreads) sdg[i] = Sr[i * m + i];
-      __syncthreads();
-      each_ij<MB>(team, m,
-          [&](int i, int j, int e) {
-            const int et = j * m + i;
-            return D6{T2[e], T2[et], Gw ? Gw[e] : 0.0, Gw ? Gw[et] : 0.0, Sr[e], Qm[e] * Si[e]};
-          },
-          [&](int i, int j, int e, const D6& v) {
-            const double g = ((v.y - v.x) + (v.z - v.w)) / 2;
-            double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * Pm[e] * v.u + 2.0 * v.d;
-            if (!(dn > 0.0)) dn = 1.0;
-            if (i == j) dn = 1.0;
-            Dn[e] = dn;
-            Rr[e] = g;
-            Mu[e] = 0.0;
-            const double z = g / dn;
-            Pp[e] = z;
-            gn2 += g * g;
-            rz += g * z;
-          });
-    }
+    each_ij<MB>(team, m,
+        [&](int i, int j, int e) {
+          const int et = j * m + i;
+          return D6{T2[e], T2[et], Gw ? Gw[e] : 0.0, Gw ? Gw[et] : 0.0, Sr[e], Qm[e] * Si[e]};
+        },
+        [&](int i, int j, int e, const D6& v) {
+          const double g = ((v.y - v.x) + (v.z - v.w)) / 2;
+          double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * Pm[e] * v.u + 2.0 * v.d;
+          if (!(dn > 0.0)) dn = 1.0;
+          if (i == j) dn = 1.0;
+          Dn[e] = dn;
+          Rr[e] = g;
+          Mu[e] = 0.0;
+          const double z = g / dn;
+          Pp[e] = z;
+          gn2 += g * g;
+          rz += g * z;
+        });
     team.sum2(gn2, rz);
     const double gnorm = sqrt(gn2);
     if (!isfinite(gnorm) || !isfinite(rz)) status = SSN_INSTANCE_NONFINITE;
@@ -985,16 +1008,17 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
         auto epi = [&](int o, int i, int j, double v) { (o == 0 ? T1 : T2)[i * m + j] = v; };
         eng.template mul<1, 2, 2, C_SHARED_A>(A, B, epi);
       }
-      __syncthreads();
+      team.sync();
       {
         MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
         MatOp B[2] = {op_n(T1, m), op_n(T2, m)};
-        auto epi = [&](int, int i, int j, double v) { Zs[i * zld + j] = v; };
+        const int zr0 = team.r0;
+        auto epi = [&](int, int i, int j, double v) { Zs[(i - zr0) * zld + j] = v; };
         eng.template mul<2, 2, 1, C_DIFF>(A, B, epi);
       }
-      __syncthreads();
+      team.sync();
       double curv = 0.0;
-      each_ij<MB>(team, m, [&](int i, int j, int e) { return D3{Pp[e], Zs[i * zld + j], Zs[j * zld + i]}; },
+      each_ij<MB>(team, m, [&](int i, int j, int e) { return D3{Pp[e], zval(i, j), zval(j, i)}; },
           [&](int, int, int, const D3& v) { curv += v.x * (v.y - v.z); });
       curv = team.sum(curv);
       if (!(curv > 0.0)) {            // H is positive definite at a strict dual optimum
@@ -1004,7 +1028,7 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
       const double alpha = rz / curv;
       double rn2 = 0.0, rz_next = 0.0;
       each_ij<MB>(team, m,
-          [&](int i, int j, int e) { return D6{Zs[i * zld + j], Zs[j * zld + i], Mu[e], Pp[e], Rr[e], Dn[e]}; },
+          [&](int i, int j, int e) { return D6{zval(i, j), zval(j, i), Mu[e], Pp[e], Rr[e], Dn[e]}; },
           [&](int, int, int e, const D6& v) {
             Mu[e] = v.z + alpha * v.w;
             const double r = v.u - alpha * (v.x - v.y);
@@ -1018,65 +1042,81 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
       rz = rz_next;
       each_ij<MB>(team, m, [&](int, int, int e) { return D3{Rr[e], Dn[e], Pp[e]}; },
           [&](int, int, int e, const D3& v) { Pp[e] = v.x / v.y + beta * v.z; });
-      __syncthreads();
+      team.sync();
     }
     // N = 2i K mu K: U = [P mu, Q mu]; K mu K = (U1 P - U2 Q) + i (U1 Q + U2 P)
-    {
-      MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
-      MatOp B[1] = {op_n(Mu, m)};
-      auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Y1 : Y2)[i * m + j] = v; };
-      eng.template mul<2, 1, 2, C_SHARED_B>(A, B, epi);
-    }
-    __syncthreads();
-    {
-      MatOp A[2] = {op_n(Y1, m), op_n(Y2, m)};
-      MatOp B[2] = {op_n(Pm, m), op_n(Qm, m)};
-      // Nr = -2 Im(K mu K), Ni = 2 Re(K mu K); Pn = Nr^T, Qn = -Ni^T
-      auto epi = [&](int o, int i, int j, double v) {
-        if (o == 0) Qn[j * m + i] = -2.0 * v;
-        else Pn[j * m + i] = -2.0 * v;
-      };
-      eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
+    // (only for a converged solve: a failed one writes NaN below, row by row)
+    if (status == SSN_INSTANCE_CONVERGED) {
+      {
+        MatOp A[2] = {op_n(Pm, m), op_n(Qm, m)};
+        MatOp B[1] = {op_n(Mu, m)};
+        auto epi = [&](int o, int i, int j, double v) { (o == 0 ? Y1 : Y2)[i * m + j] = v; };
+        eng.template mul<2, 1, 2, C_SHARED_B>(A, B, epi);
+      }
+      __syncthreads();
+      {
+        MatOp A[2] = {op_n(Y1, m), op_n(Y2, m)};
+        MatOp B[2] = {op_n(Pm, m), op_n(Qm, m)};
+        // Nr = -2 Im(K mu K), Ni = 2 Re(K mu K); Pn = Nr^T, Qn = -Ni^T
+        auto epi = [&](int o, int i, int j, double v) {
+          if (o == 0) Qn[j * m + i] = -2.0 * v;
+          else Pn[j * m + i] = -2.0 * v;
+        };
+        eng.template mul<2, 2, 2, C_SANDF>(A, B, epi);
+      }
     }
   }
   if (status != SSN_INSTANCE_CONVERGED) {
     __syncthreads();
-    for (int e = threadIdx.x; e < mm; e += kThreads) {
+    SSN_FOR_IJ(team, m, {
       Pn[e] = NAN;
       Qn[e] = NAN;
-    }
+    })
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && rank == 0) {
     a.status[inst] = status;
     if (a.cg_iters) a.cg_iters[inst] = iters;
   }
+  if constexpr (CL == 2) cg::this_cluster().sync();   // no CTA leaves while its peer may read its shared memory
 }
 
-size_t adjoint_smem_bytes(int m) {
-  const int MB = bucket_of(m);
-  const int region = MB == 1 ? dual_region_doubles(1, 1) : MB == 2 ? dual_region_doubles(2, 1)
-                   : MB == 3 ? dual_region_doubles(3, 1) : dual_region_doubles(4, 1);
-  return sizeof(double) * ((size_t)region + 2 * kWarps + 16 + 2 * kMaxM) + 16;
+size_t adjoint_smem_bytes(int MB, int CL) {
+  return sizeof(double) * ((size_t)dual_region_doubles(MB, CL) + 2 * kWarps + 16 + 2 * kMaxM) + 16;
 }
 
-cudaError_t launch_adjoint(const AdjointArgs& args, int batch, cudaStream_t stream) {
-  const size_t smem = adjoint_smem_bytes(args.m);
-  cudaError_t err = cudaSuccess;
-#define SSN_ADJ_CASE(MBV)                                                                              \
-  case MBV:                                                                                            \
-    err = cudaFuncSetAttribute(adjoint_kernel<MBV>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
-                               static_cast<int>(smem));                                               \
-    if (err != cudaSuccess) return err;                                                                \
-    adjoint_kernel<MBV><<<batch, kThreads, smem, stream>>>(args);                                      \
-    break;
-  switch (bucket_of(args.m)) {
-    SSN_ADJ_CASE(1)
-    SSN_ADJ_CASE(2)
-    SSN_ADJ_CASE(3)
-    SSN_ADJ_CASE(4)
-  }
-#undef SSN_ADJ_CASE
+template <int MB, int CL>
+static cudaError_t launch_adjoint_mb(const AdjointArgs& args, int batch, cudaStream_t stream) {
+  const size_t smem = adjoint_smem_bytes(MB, CL);
+  cudaError_t err = cudaFuncSetAttribute(adjoint_kernel<MB, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(batch * CL);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  err = cudaLaunchKernelEx(&cfg, adjoint_kernel<MB, CL>, args);
+  if (err != cudaSuccess) return err;
   return cudaGetLastError();
+}
+
+// One CTA per instance, or a 2-CTA cluster when the batch leaves SMs idle (the rule of
+// the Newton kernel).
+cudaError_t launch_adjoint(const AdjointArgs& args, int batch, cudaStream_t stream) {
+  const bool two = dual_cluster_size(batch, args.m) == 2;
+  switch (bucket_of(args.m)) {
+    case 1: return launch_adjoint_mb<1, 1>(args, batch, stream);
+    case 2: return two ? launch_adjoint_mb<2, 2>(args, batch, stream) : launch_adjoint_mb<2, 1>(args, batch, stream);
+    case 3: return two ? launch_adjoint_mb<3, 2>(args, batch, stream) : launch_adjoint_mb<3, 1>(args, batch, stream);
+    default: return two ? launch_adjoint_mb<4, 2>(args, batch, stream) : launch_adjoint_mb<4, 1>(args, batch, stream);
+  }
 }
 
 // ---------------------------------------------------------------- SPD inverse component
