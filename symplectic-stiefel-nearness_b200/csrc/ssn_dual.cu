@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           const double beta = rz_next / rz;
           each_ij<MB>(team, m, [&](int i, int j, int e) { return D3{Rr[e], den(i, j, e), Pp[e]}; },
               [&](int, int, int e, const D3& v) { Pp[e] = __dadd_rn(__ddiv_rn(v.x, v.y), __dmul_rn(beta, v.z)); });
-          team.sync();
+          __syncthreads();   // the next HVP reads only this CTA's rows of p (its A operand)
           rz = rz_next;
         }
         double sl = 0.0;
@@ -1042,7 +1042,7 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
       rz = rz_next;
       each_ij<MB>(team, m, [&](int, int, int e) { return D3{Rr[e], Dn[e], Pp[e]}; },
           [&](int, int, int e, const D3& v) { Pp[e] = v.x / v.y + beta * v.z; });
-      team.sync();
+      __syncthreads();       // the next HVP reads only this CTA's rows of p; mu was published by sum2
     }
     // N = 2i K mu K: U = [P mu, Q mu]; K mu K = (U1 P - U2 Q) + i (U1 Q + U2 P)
     // (only for a converged solve: a failed one writes NaN below, row by row)
