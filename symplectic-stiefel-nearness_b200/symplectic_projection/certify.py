@@ -80,3 +80,40 @@ def certify(T: torch.Tensor, X: torch.Tensor) -> dict:
     passed = finite & (feas <= THRESHOLDS["feasibility"]) & (stat <= THRESHOLDS["stationarity"]) \
         & (delta <= THRESHOLDS["delta"])
     return {"feasibility": feas, "stationarity": stat, "delta": delta, "passed": passed}
+
+
+@torch.no_grad()
+def solve_certified(T: torch.Tensor, precision: str = "split", fallback: str | None = "fp64", **options):
+    """Solve, certify every instance on the device, and rerun the ones that fail.
+
+    T is a CUDA float64 [batch, 2n, 2k].  The batch is solved in ``precision``
+    (options as for ``solve_ex``) and certified with the reference's acceptance
+    test.  Instances that did not converge or do not pass are solved again, alone
+    as one smaller batch, in the ``fallback`` form (None: no rerun); a rerun result
+    replaces the first one only where it passes.  The two forms take different
+    Newton paths, so on ill-conditioned batches they tend to miss different
+    instances.  Returns (X, omega, iterations, report) with report holding the
+    per-instance metrics, ``passed``, and the indices that were rerun.
+    """
+    from .dual_recommended_hvp import solve_ex
+    res = solve_ex(T, precision=precision, **options)
+    X, omega, iterations = res.X, res.omega, res.iterations.clone()
+    cert = certify(T, X)
+    passed = cert["passed"] & (res.status == 0)
+    rerun = (~passed).nonzero().flatten()
+    if fallback is not None and rerun.numel() > 0:
+        sub = solve_ex(T[rerun].contiguous(), precision=fallback, **options)
+        sub_cert = certify(T[rerun].contiguous(), sub.X)
+        ok = sub_cert["passed"] & (sub.status == 0)
+        take = rerun[ok]
+        if take.numel() > 0:
+            X[take] = sub.X[ok]
+            omega[take] = sub.omega[ok]
+            iterations[take] = sub.iterations[ok]
+            for key in ("feasibility", "stationarity", "delta"):
+                cert[key][take] = sub_cert[key][ok]
+            passed[take] = True
+    report = {key: cert[key] for key in ("feasibility", "stationarity", "delta")}
+    report["passed"] = passed
+    report["rerun"] = rerun
+    return X, omega, iterations, report

@@ -82,3 +82,21 @@ def test_config5_width_illconditioned(sp, precision):
     assert res.status.cpu().tolist() == [0, 0]
     for rec in O.inspect_output(T, res.X.cpu()):
         assert O.passes(rec), rec
+
+
+def test_certified_solve_reruns_failures_in_the_other_form(sp):
+    """solve_certified: passing instances keep the first form's result; a failure is
+    rerun in the fallback form and replaced only where that passes."""
+    from symplectic_projection.certify import solve_certified
+    from symplectic_projection.inputs import illcond_targets
+    T = torch.cat((O.make_inputs(64, 4, 0, 2)[0], illcond_targets(64, 4, 2))).cuda()
+    X, W, it, rep = solve_certified(T, precision="split", fallback="fp64", preconditioner="adaptive")
+    assert rep["passed"].all()
+    ref = sp.solve_ex(T, precision="split", preconditioner="adaptive")
+    keep = [i for i in range(4) if i not in rep["rerun"].tolist()]
+    assert torch.equal(X[keep], ref.X[keep])
+    for rec in O.inspect_output(T.cpu(), X.cpu()):
+        assert O.passes(rec), rec
+    # a forced cap fails every instance; with no fallback nothing is rerun
+    X2, _, _, rep2 = solve_certified(T, precision="split", fallback=None, max_newton=1)
+    assert not rep2["passed"].any() and rep2["rerun"].tolist() == [0, 1, 2, 3]
