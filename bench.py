@@ -8,10 +8,13 @@ r_F <= 1e-8, r_G <= 1e-9, delta <= 1e-8 (checked on the device after timing).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun, one rank per GPU, each rank solving its own batch
+N > 1 runs one rank per GPU under torchrun, each rank solving its own batch
 (weak scaling, no collective on the data path); the step time is the max over
-ranks.  ``--impl reference`` times the reference algorithm's CPU FP64 path (the
-CPU restatement in oracle/, all host threads) on the same workload.
+ranks.  Started without torchrun, ``--gpus N`` (N > 1) re-executes itself under
+``torch.distributed.run`` with N ranks; started by torchrun, the world size
+must equal N.  ``--impl reference`` times the reference algorithm's CPU FP64
+path (the CPU restatement in oracle/, all host threads) on the same workload;
+under torchrun rank 0 alone runs it.
 """
 from __future__ import annotations
 
@@ -63,7 +66,7 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--n", type=int, default=N_DEFAULT)
+    p.add_argument("--n", "--size-n", dest="n", type=int, default=N_DEFAULT)
     p.add_argument("--k", type=int, default=K_DEFAULT)
     p.add_argument("--batch", type=int, default=BATCH_DEFAULT)
     p.add_argument("--e2e-steps", type=int, default=5)
@@ -129,10 +132,10 @@ def run_reference(args):
     sys.path.insert(0, str(ROOT))
     from oracle import ssn_oracle as O
     T, _ = O.make_inputs(args.n, args.k, 5 if (args.n, args.k) == (4096, 48) else 0, args.batch)
-    for _ in range(max(0, min(args.warmup, 1))):
+    for _ in range(max(0, args.warmup)):
         O.solve(T)
     times = []
-    steps = max(1, min(args.steps, 5))               # each step is a full batch: bounded run time
+    steps = max(1, args.steps)                       # each step is one full batched solve of the workload
     for _ in range(steps):
         t0 = time.perf_counter()
         O.solve(T)
@@ -141,7 +144,8 @@ def run_reference(args):
     value = args.batch * steps / total
     threads = torch.get_num_threads()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * total / steps,
+            "ranks_launched": int(os.environ.get("WORLD_SIZE", "1")),
+            "steps": steps, "warmup": max(0, args.warmup), "ms_per_step": 1e3 * total / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded N(0,1/(2n)) targets (reference generator rule)",
             "config": workload(args),
@@ -730,8 +734,31 @@ def run_illcond(args):
     return 0 if passed else 1
 
 
+def free_port() -> int:
+    import socket
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        return sock.getsockname()[1]
+
+
+def launch_ranks(nproc: int, argv, script=None, limit_s: int = 1800) -> int:
+    """Run ``script argv`` as ``nproc`` ranks under torch.distributed.run on 127.0.0.1 and
+    return its exit code; ``timeout -k 60`` bounds the whole job."""
+    # torchrun's parser rejects script options that abbreviate its own (--n: --nnodes, --nproc...)
+    argv = ["--size-n" if a == "--n" else ("--size-n=" + a[4:] if a.startswith("--n=") else a) for a in argv]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()),
+           str(script or Path(__file__).resolve()), *argv]
+    return subprocess.call(["timeout", "-k", "60", str(limit_s), *cmd])
+
+
 def main():
     args = parse()
+    world = os.environ.get("WORLD_SIZE")
+    if world is None and args.gpus > 1:
+        return launch_ranks(args.gpus, sys.argv[1:])
+    if world is not None and int(world) != args.gpus:
+        raise SystemExit(f"bench.py: WORLD_SIZE={world} but --gpus {args.gpus}; launch one rank per GPU")
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "ragged":

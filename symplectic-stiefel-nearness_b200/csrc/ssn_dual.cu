@@ -474,10 +474,18 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
             sdg[i] = Sr[i * m + i];
           }
           __syncthreads();
-          each_ij<MB>(team, m, [&](int, int, int e) { return D4{Pm[e], Sr[e], Qm[e], Si[e]}; },
+          // Both (i, j) and (j, i) evaluate the same expression on the upper-triangle entries
+          // (a, b) = (min, max), so the denominators are exactly symmetric and r / den stays
+          // exactly antisymmetric: the CG directions, trials and omega keep exact skewness.
+          each_ij<MB>(team, m,
+              [&](int i, int j, int) {
+                const int eu = imin(i, j) * m + imax(i, j);
+                return D4{Pm[eu], Sr[eu], Qm[eu], Si[eu]};
+              },
               [&](int i, int j, int e, const D4& v) {
-                double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * v.x * v.y + 2.0 * v.z * v.w;
-                if (!(dn > 0.0)) dn = lam[i] + lam[j];   // only off-diagonal entries matter; keep them positive
+                const int a0 = imin(i, j), b0 = imax(i, j);
+                double dn = pdg[a0] * sdg[b0] + pdg[b0] * sdg[a0] - 2.0 * v.x * v.y + 2.0 * v.z * v.w;
+                if (!(dn > 0.0)) dn = lam[a0] + lam[b0];   // only off-diagonal entries matter; keep them positive
                 Dn[e] = i == j ? 1.0 : dn;
               });
         }
@@ -762,15 +770,7 @@ static size_t dual_smem_bytes(int MB, int CL) {
   return sizeof(double) * ((size_t)region + 2 * kWarps + 3 * kMaxM + 8) + 16;
 }
 
-static int sm_count() {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-  }
-  return sms;
-}
+static int sm_count() { return current_device_sm_count(); }
 
 template <int MB, int CL>
 static cudaError_t launch_dual_mb(const DualArgs& args, int batch, cudaStream_t stream) {
@@ -976,11 +976,14 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjointArgs a) {
     each_ij<MB>(team, m,
         [&](int i, int j, int e) {
           const int et = j * m + i;
-          return D6{T2[e], T2[et], Gw ? Gw[e] : 0.0, Gw ? Gw[et] : 0.0, Sr[e], Qm[e] * Si[e]};
+          // the denominator from the upper-triangle entries: exactly symmetric, so mu stays skew
+          const int eu = imin(i, j) * m + imax(i, j);
+          return D6{T2[e], T2[et], Gw ? Gw[e] : 0.0, Gw ? Gw[et] : 0.0, Pm[eu] * Sr[eu], Qm[eu] * Si[eu]};
         },
         [&](int i, int j, int e, const D6& v) {
           const double g = ((v.y - v.x) + (v.z - v.w)) / 2;
-          double dn = pdg[i] * sdg[j] + pdg[j] * sdg[i] - 2.0 * Pm[e] * v.u + 2.0 * v.d;
+          const int a0 = imin(i, j), b0 = imax(i, j);
+          double dn = pdg[a0] * sdg[b0] + pdg[b0] * sdg[a0] - 2.0 * v.u + 2.0 * v.d;
           if (!(dn > 0.0)) dn = 1.0;
           if (i == j) dn = 1.0;
           Dn[e] = dn;

@@ -11,6 +11,8 @@
 // Recovery (replaces recover_block, recovery_fused.py:19-30, and recover_fused,
 // recovery_fused.cu:2-41): Ur = A P^T + D Q^T, Ui = D P^T - A Q^T, one CTA per
 // (row block, instance), the four products sharing fragments.
+#include <atomic>
+
 #include "ssn_common.cuh"
 #include "ssn_internal.h"
 
@@ -22,16 +24,20 @@ constexpr uint32_t C_G = coef_bit(0, 0, 1, 1);
 constexpr uint32_t C_REC = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1) | coef_bit(1, 1, 0, 1) |
                            coef_bit(1, 0, 1, 2);
 
-static int device_sm_count() {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
-      sms = 148;
+int current_device_sm_count() {
+  constexpr int kMaxDevices = 64;
+  static std::atomic<int> cache[kMaxDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 148;
+  int sms = cache[dev].load(std::memory_order_relaxed);
+  if (sms <= 0) {
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    cache[dev].store(sms, std::memory_order_relaxed);
   }
   return sms;
 }
+
+static int device_sm_count() { return current_device_sm_count(); }
 
 struct GramSplit {
   int splits, chunk;

@@ -12,6 +12,10 @@ namespace ssn {
 // Number of m x m FP64 matrices of per-instance dual workspace.
 constexpr int kDualMats = 22;
 
+// SM count of the current device, cached per device index (148 on B200; 148 if
+// the query fails).  Safe to call from several host threads.
+int current_device_sm_count();
+
 struct DualArgs {
   int m;
   int max_newton, max_cg, max_backtrack;

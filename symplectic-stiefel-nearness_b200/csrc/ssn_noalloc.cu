@@ -19,8 +19,11 @@
 //    clearing is needed; calls that overlap on the GPU (other streams, other
 //    host threads) race on it and must be serialised by the caller;
 //  * the first call on each device resolves the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; that first
-//    call should come before any stream capture.
+//    cudaGetSymbolAddress (with that device current) and caches it per device
+//    index for the life of the process; that first call should come before any
+//    stream capture.  Resetting the device or recreating its primary context
+//    (cudaDeviceReset) while the library stays loaded is not supported: the
+//    cached address would then be stale.
 #include <mutex>
 
 #include "ssn_common.cuh"

@@ -505,15 +505,7 @@ struct OzGramPlan {
   int chunk, nchunks, ncg;
 };
 
-int sm_count_oz() {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-  }
-  return sms;
-}
+int sm_count_oz() { return current_device_sm_count(); }
 
 // Row chunks per instance: the count minimising waves x chunk length (one CTA per
 // SM), chunks a multiple of the pre-pass block and short enough for exact INT32.

@@ -84,6 +84,42 @@ def test_config5_width_illconditioned(sp, precision):
         assert O.passes(rec), rec
 
 
+@pytest.mark.parametrize("precision", ["split", "fp64"])
+def test_stress_instance_19_alone_at_full_size(sp, precision):
+    """Target 19 of the stress batch (32768 x 128, Gram condition ~1e8) solved alone: it
+    converges and passes the acceptance test in both forms, with no rerun."""
+    from symplectic_projection.inputs import illcond_targets
+    T = illcond_targets(16384, 64, 20)[19:20].contiguous()
+    res = sp.solve_ex(T.cuda(), precision=precision, preconditioner="adaptive")
+    assert res.status.cpu().tolist() == [0]
+    for rec in O.inspect_output(T, res.X.cpu()):
+        assert O.passes(rec), rec
+
+
+@pytest.mark.parametrize("precision", ["split", "fp64"])
+def test_adaptive_solution_is_a_consistent_inverse_pair(sp, precision):
+    """With the adaptive preconditioner the returned P, Q stay an exact inverse pair of
+    I + i omega: P symmetric, and P = (I + omega^2)^-1, Q = -omega P to rounding.  (X = T K^-1
+    is then stationary, whatever the Gram's error.)"""
+    from symplectic_projection import dual_recommended_hvp as D
+    from symplectic_projection.gram_triangle_reflect import gram
+    from symplectic_projection.inputs import illcond_targets
+    T = illcond_targets(2048, 64, 2, seed=2026102501).cuda()
+    n = T.shape[1] // 2
+    Cr, Ci = gram(T[:, :n], T[:, n:], precision=precision)
+    final = []
+    W, _, _ = D.dual_batch(Cr, Ci, final, precision=precision, preconditioner="adaptive")
+    P, Q = (x.cpu() for x in final)
+    W = W.cpu()
+    eye = torch.eye(W.shape[-1], dtype=torch.float64)
+    for b in range(W.shape[0]):
+        Pn = torch.linalg.norm(P[b])
+        assert torch.linalg.norm(P[b] - P[b].mT) / Pn < 1e-12
+        Pi = torch.linalg.inv(eye + W[b] @ W[b])
+        assert torch.linalg.norm(P[b] - Pi) / Pn < 1e-10
+        assert torch.linalg.norm(Q[b] + W[b] @ P[b]) / Pn < 1e-10
+
+
 def test_certified_solve_reruns_failures_in_the_other_form(sp):
     """solve_certified: passing instances keep the first form's result; a failure is
     rerun in the fallback form and replaced only where that passes."""
