@@ -57,12 +57,15 @@ enum {
   /* Plain FP64 throughout: the reference's algorithm step for step (same
    * iterates up to rounding), with a fully converged FP64 Jacobi eigenbasis. */
   SSN_PRECISION_FP64 = 0,
-  /* Split precision: the eigenbasis of the scaled Gram comes from a few FP32
+  /* Split precision: the Gram and the recovery are INT8 Ozaki products on the
+   * tensor cores; the eigenbasis of the scaled Gram comes from a few FP32
    * Jacobi sweeps (ssn_options.eig_sweeps), is re-orthogonalised in FP64, and
    * the Newton iteration uses the full rotated Gram, so the solution is the
-   * same dual optimum; Newton, line search and residuals stay FP64.  Inputs
-   * and outputs are FP64 and every result is held to the same acceptance
-   * bounds as the FP64 form. */
+   * same dual optimum.  The early Newton steps run in FP32
+   * (ssn_options.fp32_newton); the last Newton step(s), their line search and
+   * positive-definiteness test, and the residual that declares convergence
+   * are FP64.  Inputs and outputs are FP64 and every result is held to the
+   * same acceptance bounds as the FP64 form. */
   SSN_PRECISION_SPLIT = 1
 };
 
@@ -77,7 +80,11 @@ typedef struct {
                         no sweep when every off-diagonal correlation of the scaled Gram is
                         below 0.1 (identity basis), else 1 */
   int preconditioner; /* SSN_PRECOND_EIGENBASIS (default) or SSN_PRECOND_ADAPTIVE */
-  int reserved[5];
+  int fp32_newton;   /* split form: 0 (default) or 1 run the early Newton steps in FP32 where
+                        their state fits on chip (m <= 64, or m <= 96 with two CTAs per
+                        instance), until the FP32 residual is below 1e-5; -1 keeps every
+                        Newton step in FP64.  Ignored by the FP64 form. */
+  int reserved[4];
 } ssn_options;
 
 /* CG preconditioner (ssn_options.preconditioner). */
@@ -245,8 +252,10 @@ int ssn_dual(const double* Cr, const double* Ci, double* omega, double* P, doubl
 /*
  * The Newton-CG part of ssn_dual alone, given the eigendecomposition from
  * ssn_eigh (values, vectors, scale, and its per-instance status eig_status,
- * which may be NULL).  counters (may be NULL) receives int32 [batch, 4]:
- * Newton steps run, Hessian-vector products, line-search trials, fallbacks.
+ * which may be NULL).  counters (may be NULL) receives int32 [batch, 8]:
+ * Newton steps run, Hessian-vector products, line-search trials and fallbacks
+ * of the FP64 iteration, then the same four of the split form's FP32 phase
+ * (zeros when it does not run).
  * Cr (the unscaled Gram) is read only with the full rotated Gram (the split
  * form, or the adaptive preconditioner), where it is required; it may be NULL
  * otherwise.
@@ -259,6 +268,16 @@ int ssn_newton(const double* Cr, const double* Ci, const double* values, const d
                int64_t* iterations, int32_t* status, int32_t* counters, int batch, int m,
                void* workspace, size_t workspace_bytes, const ssn_options* opt,
                ssn_stream_t stream);
+
+/*
+ * Measurement helper with no counterpart in the reference.  While set, every
+ * Newton-CG run started from the calling host thread (ssn_newton, ssn_dual,
+ * ssn_solve) records events[0..3] on its stream: before the basis set-up,
+ * before the split form's FP32 Newton phase, before the FP64 iteration, and
+ * after it (events[1] and [2] coincide when no FP32 phase runs).  events: four
+ * cudaEvent_t handles owned by the caller; NULL stops the recording.
+ */
+int ssn_set_newton_events(void* const* events);
 
 /*
  * Measurement helper with no counterpart in the reference: launches a

@@ -146,6 +146,8 @@ void fill_options(const ssn_options* opt, DualArgs& a) {
   // its four m x m products for FP64 ones too, whose ~1e-14 residue ill-conditioned targets
   // (an inverse of norm ~1e2 in P + iQ) amplify into the primal's stationarity
   a.orthogonalize = a.approx_basis;
+  // split form: the early Newton steps in FP32 unless the caller keeps them FP64
+  a.fp32_newton = (split && opt->fp32_newton >= 0) ? 1 : 0;
 }
 
 bool split_form(const ssn_options* opt) { return opt && opt->precision == SSN_PRECISION_SPLIT; }
@@ -157,7 +159,7 @@ bool options_ok(const ssn_options* opt) {
          opt->max_cg <= 100000 && opt->max_backtrack >= 1 && opt->max_backtrack <= 1074 &&
          opt->feas_tol > 0.0 &&
          (opt->precision == SSN_PRECISION_FP64 || opt->precision == SSN_PRECISION_SPLIT) &&
-         opt->eig_sweeps >= 0 && opt->eig_sweeps <= 24 &&
+         opt->eig_sweeps >= 0 && opt->eig_sweeps <= 24 && opt->fp32_newton >= -1 && opt->fp32_newton <= 1 &&
          (opt->preconditioner == SSN_PRECOND_EIGENBASIS || opt->preconditioner == SSN_PRECOND_ADAPTIVE);
 }
 
@@ -430,6 +432,11 @@ int ssn_newton(const double* Cr, const double* Ci, const double* values, const d
   a.status = status;
   a.counters = counters;
   return cuda_status(launch_dual(a, batch, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_set_newton_events(void* const* events) {
+  set_newton_events(events);
+  return SSN_OK;
 }
 
 int ssn_probe_fp64_mma(double* sink, int iters, double* flops, ssn_stream_t stream) {

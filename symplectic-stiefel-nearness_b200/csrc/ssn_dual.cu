@@ -30,9 +30,13 @@ namespace ssn {
 
 enum Mat {
   M_CE = 0, M_JE, M_W, M_WT, M_P, M_PT, M_Q, M_SR, M_SI, M_G, M_D, M_R, M_PP, M_HP, M_DL,
-  M_T1, M_T2, M_T3, M_X0, M_X1, M_X2, M_DEN
+  M_T1, M_T2, M_T3, M_X0, M_X1, M_X2, M_DEN, M_AUX
 };
-static_assert(M_DEN + 1 == kDualMats, "workspace matrix count");
+static_assert(M_AUX + 1 == kDualMats, "workspace matrix count");
+// The FP32 phase (ssn_dual32.cu) reads the set-up from, and writes its omega and counters
+// to, these slots; it uses M_T1..M_T3 as scratch.
+static_assert(M_CE == 0 && M_JE == 1 && M_W == 2 && M_T1 == 15 && M_X2 == 20 && M_AUX == 22,
+              "slots shared with the FP32 phase");
 
 constexpr uint32_t C_ONE = coef_bit(0, 0, 0, 1);
 constexpr uint32_t C_SHARED_B = coef_bit(0, 0, 0, 1) | coef_bit(1, 1, 0, 1);
@@ -207,6 +211,8 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
   int* flag = reinterpret_cast<int*>(xch + 8);
   int* vflag = flag + 1;                      // cluster: the trial inverse's outcome, written by CTA 0
   int* vflag_peer = vflag;
+  int* perm_col = flag + 2;                   // kMaxM: permutation basis, V[perm_col[a]][a] = 1
+  int* perm_row = perm_col + kMaxM;           // kMaxM: V[r][perm_row[r]] = 1
   double* Zs = smem;                          // this CTA's rows of the HVP outer product
   const int zld = m + 1;
 
@@ -269,12 +275,68 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
 
   int64_t iterations = 0;
   int n_hvp = 0, n_trial = 0, n_fallback = 0, n_step = 0;
+  const int32_t* aux = reinterpret_cast<const int32_t*>(ws + (size_t)M_AUX * mm);   // the FP32 phase's counts
   if (status == SSN_INSTANCE_CONVERGED) {
+    double* CrE = ws + (size_t)M_X2 * mm;       // approximate basis: sym(V^T (Cr/s) V)
+    const bool approx = a.approx_basis != 0;
+    // (the same bits for both CTAs of a cluster, so both take the same branch and barriers)
+    const bool refine_basis = a.approx_basis && a.orthogonalize && !(a.sweeps && a.sweeps[inst] == 0);
+    // A basis from no Jacobi sweep is a permutation (the identity in eigenvalue order), exact
+    // in FP64: the basis changes of the set-up and the exit are then gathers, not products.
+    const bool perm = a.sweeps && a.sweeps[inst] == 0;
+    if (perm) {
+      for (int r = threadIdx.x; r < m; r += kThreads) {
+        int c = 0;
+        for (int j = 0; j < m; ++j)
+          if (V[(size_t)r * m + j] != 0.0) c = j;
+        perm_row[r] = c;
+        perm_col[c] = r;
+      }
+      __syncthreads();
+    }
+    if (a.phase == 2) {
+      // the set-up of the phase-1 launch is in the workspace: Ce, Je, CrE (and Sr = CrE),
+      // the refined basis in M_X1; omega, P = I, Q = 0 (omega since rewritten by the FP32 phase)
+      if (refine_basis) V = ws + (size_t)M_X1 * mm;
+      if (approx) {
+        for (int i = threadIdx.x; i < m; i += kThreads) lam[i] = CrE[i * m + i];
+        __syncthreads();
+      }
+    } else if (perm) {
+      // V^T X V = X[c][c'] with c = perm_col: the same values the products give, gathered.
+      // J(V)[r][b] = V[r + h][b] (r < h) or -V[r - h][b], so (V^T J(V))[a][b] = +-1 where
+      // b = perm_row[perm_col[a] +- h].
+      const int h = m / 2;
+      const double* Crb = a.Cr + (size_t)inst * mm;
+      auto jv = [&](int a0, int b0) -> double {
+        const int r = perm_col[a0];
+        return r < h ? (perm_row[r + h] == b0 ? 1.0 : 0.0) : (perm_row[r - h] == b0 ? -1.0 : 0.0);
+      };
+      SSN_FOR_IJ(team, m, {
+        const int pa = perm_col[i];
+        const int pb = perm_col[j];
+        Ce[e] = (Ci[pa * m + pb] / s - Ci[pb * m + pa] / s) / 2;
+        Je[e] = ((jv(i, j) - jv(j, i)) / 2) / s;
+        if (approx) {
+          const double c = (Crb[pa * m + pb] / s + Crb[pb * m + pa] / s) / 2;
+          CrE[e] = c;
+          Sr[e] = c;
+        } else {
+          Sr[e] = (i == j) ? lam[i] : 0.0;
+        }
+        Wm[e] = 0.0;
+        Pm[e] = (i == j) ? 1.0 : 0.0;
+        Qm[e] = 0.0;
+      })
+      team.sync();
+      if (approx) {
+        for (int i = threadIdx.x; i < m; i += kThreads) lam[i] = CrE[i * m + i];
+        __syncthreads();
+      }
+    } else {
     // ---- eigenbasis set-up: Ce = skew(V^T (Ci/s) V), Je = skew(V^T J(V)) / s  (:106-111, :53-56)
     const int h = m / 2;
-    double* CrE = ws + (size_t)M_X2 * mm;       // approximate basis: sym(V^T (Cr/s) V)
-    // (the same bits for both CTAs of a cluster, so both take the same branch and barriers)
-    if (a.approx_basis && a.orthogonalize && !(a.sweeps && a.sweeps[inst] == 0)) {
+    if (refine_basis) {
       // V <- V (3I - V^T V) / 2 twice: vectors from FP32 rotations become orthogonal to FP64 rounding
       double* Vb[2] = {ws + (size_t)M_X2 * mm, ws + (size_t)M_X1 * mm};
       const double* Vin = V;
@@ -361,7 +423,6 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
     // Skew parts are exactly antisymmetric ((x - y)/2 vs (y - x)/2), which every
     // later pass relies on: precondition(r) = r / den and skew(w + t d) = w + t d
     // hold bit for bit for exactly skew r, w, d.
-    const bool approx = a.approx_basis != 0;
     each_ij<MB>(team, m,
         [&](int i, int j, int e) {
           const int et = j * m + i;
@@ -376,11 +437,81 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
           if (!approx) Sr[e] = (i == j) ? lam[i] : 0.0;
         });
     team.sync();
+    }
+    if (a.phase == 1) {
+      if constexpr (CL == 2) cg::this_cluster().sync();   // no CTA leaves while its peer may read it
+      return;
+    }
+
+    // ---- warm start from the FP32 phase: P = (I + omega^2)^-1 in FP64 with the
+    // positive-definiteness test, then the iteration continues at a general step
+    int warm = 0, step0 = 0;
+    if (a.phase == 2 && aux[0] > 0) {
+      warm = aux[0];
+      double* Ks = smem;
+      const int mp16 = round_up(m, 16), kld = frag_ld(mp16);
+      bool valid;
+      if constexpr (CL == 1) {
+        {
+          MatOp A[1] = {op_n(Wm, m)};
+          MatOp B[1] = {op_n(Wm, m)};
+          auto epi = [&](int, int i, int j, double v) { Ks[i * kld + j] = __dadd_rn(i == j ? 1.0 : 0.0, v); };
+          eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+        }
+        for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {   // identity padding up to mp16
+          const int i = e / mp16, j = e - i * mp16;
+          if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
+        }
+        __syncthreads();
+        valid = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
+        if (valid) {
+          SSN_FOR_IJ(team, m, { Pm[e] = Ks[i * kld + j]; })
+        }
+        __syncthreads();
+      } else {
+        {
+          MatOp A[1] = {op_n(Wm, m)};
+          MatOp B[1] = {op_n(Wm, m)};
+          auto epi = [&](int, int i, int j, double v) { Kg[i * m + j] = __dadd_rn(i == j ? 1.0 : 0.0, v); };
+          eng.template mul<1, 1, 1, C_ONE>(A, B, epi);
+        }
+        team.sync();
+        if (rank == 0) {
+          for (int i = (int)(threadIdx.x >> 5); i < m; i += kWarps)
+            for (int j = (int)(threadIdx.x & 31); j < m; j += 32) Ks[i * kld + j] = Kg[i * m + j];
+          for (int e = threadIdx.x; e < mp16 * mp16; e += kThreads) {
+            const int i = e / mp16, j = e - i * mp16;
+            if (i >= m || j >= m) Ks[i * kld + j] = (i == j) ? 1.0 : 0.0;
+          }
+          __syncthreads();
+          const bool ok = spd_inverse_blocked(Ks, mp16, kld, Ks + mp16 * kld, flag);
+          if (threadIdx.x == 0) {
+            vflag[0] = ok ? 1 : 0;
+            vflag_peer[0] = ok ? 1 : 0;
+          }
+          if (ok)
+            for (int i = (int)(threadIdx.x >> 5); i < m; i += kWarps)
+              for (int j = (int)(threadIdx.x & 31); j < m; j += 32) Pm[i * m + j] = Ks[i * kld + j];
+        }
+        team.sync();
+        valid = *reinterpret_cast<volatile int*>(vflag) != 0;
+      }
+      if (valid) {
+        step0 = 1;
+      } else {
+        // not positive definite in FP64: start over from omega = 0 (P = I, Q = 0 from the set-up)
+        SSN_FOR_IJ(team, m, { Wm[e] = 0.0; })
+        team.sync();
+      }
+      iterations = warm;
+    }
 
     const double sqrt_m = sqrt(static_cast<double>(m));
     const double* SiCur = Ce;  // Si = Ci in the eigenbasis at step 0 (:121-122)
     bool done = false;
-    for (int step = 0; step < a.max_newton && !done && status == SSN_INSTANCE_CONVERGED; ++step) {
+    // Newton steps left for this launch: the cap counts the FP32 phase's updates too
+    for (int step = step0, left = a.max_newton - warm; left > 0 && !done && status == SSN_INSTANCE_CONVERGED;
+         ++step, --left) {
       ++n_step;
       if (step > 0) {
         // Q = -omega P (:124)
@@ -722,6 +853,16 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
     double* Pout = a.P + (size_t)inst * mm;
     double* Qout = a.Q + (size_t)inst * mm;
     team.sync();
+    if (perm) {
+      // permutation basis: (V X V^T)[r][q] = X[perm_row[r]][perm_row[q]]
+      SSN_FOR_IJ(team, m, {
+        const int oi = perm_row[i];
+        const int oj = perm_row[j];
+        Wout[e] = (Wm[oi * m + oj] - Wm[oj * m + oi]) / 2;
+        Pout[e] = Pm[oi * m + oj];
+        Qout[e] = Qm[oi * m + oj];
+      })
+    } else {
     {
       MatOp A[1] = {op_n(V, m)};
       MatOp B[2] = {op_n(Wm, m), op_n(Pm, m)};
@@ -751,15 +892,18 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
     }
     team.sync();
     SSN_FOR_IJ(team, m, { Wout[e] = (Dl[e] - Dl[j * m + i]) / 2; })
+    }
   }
   if (threadIdx.x == 0 && rank == 0) {
     a.iterations[inst] = iterations;
     a.status[inst] = status;
     if (a.counters) {
-      a.counters[inst * 4 + 0] = n_step;
-      a.counters[inst * 4 + 1] = n_hvp;
-      a.counters[inst * 4 + 2] = n_trial;
-      a.counters[inst * 4 + 3] = n_fallback;
+      a.counters[inst * 8 + 0] = n_step;
+      a.counters[inst * 8 + 1] = n_hvp;
+      a.counters[inst * 8 + 2] = n_trial;
+      a.counters[inst * 8 + 3] = n_fallback;
+      const bool f32 = a.phase == 2;
+      for (int c = 0; c < 4; ++c) a.counters[inst * 8 + 4 + c] = f32 ? aux[1 + c] : 0;
     }
   }
   if constexpr (CL == 2) cg::this_cluster().sync();   // no CTA leaves while its peer may read its shared memory
@@ -767,7 +911,7 @@ __global__ void __launch_bounds__(kThreads, 1) dual_kernel(DualArgs a) {
 
 static size_t dual_smem_bytes(int MB, int CL) {
   const int region = dual_region_doubles(MB, CL);
-  return sizeof(double) * ((size_t)region + 2 * kWarps + 3 * kMaxM + 8) + 16;
+  return sizeof(double) * ((size_t)region + 2 * kWarps + 3 * kMaxM + 8) + 16 + sizeof(int) * 2 * kMaxM;
 }
 
 static int sm_count() { return current_device_sm_count(); }
@@ -799,14 +943,69 @@ static cudaError_t launch_dual_mb(const DualArgs& args, int batch, cudaStream_t 
 // enough for the row split to pay; one otherwise.
 int dual_cluster_size(int batch, int m) { return (m >= 48 && 2 * batch <= sm_count()) ? 2 : 1; }
 
-cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
-  const bool two = dual_cluster_size(imax(batch, args.concurrent), args.m) == 2;
+static cudaError_t launch_dual_phase(const DualArgs& args, int batch, bool two, cudaStream_t stream) {
   switch (bucket_of(args.m)) {
     case 1: return launch_dual_mb<1, 1>(args, batch, stream);
     case 2: return two ? launch_dual_mb<2, 2>(args, batch, stream) : launch_dual_mb<2, 1>(args, batch, stream);
     case 3: return two ? launch_dual_mb<3, 2>(args, batch, stream) : launch_dual_mb<3, 1>(args, batch, stream);
     default: return two ? launch_dual_mb<4, 2>(args, batch, stream) : launch_dual_mb<4, 1>(args, batch, stream);
   }
+}
+
+// FP32 residual below which the split form's FP32 phase hands over to the FP64
+// iteration: FP32 resolves these residuals to about 1e-7, and from 1e-5 one FP64
+// Newton step (quadratic convergence) usually reaches the stopping tolerance.
+constexpr double kFp32SwitchTol = 1e-5;
+
+// Events recorded around the Newton launches of the calling host thread (a measurement
+// hook, ssn_set_newton_events): before the set-up, before the FP32 phase, before the FP64
+// iteration, after it.
+static thread_local cudaEvent_t t_newton_events[4] = {};
+static thread_local bool t_newton_events_set = false;
+
+void set_newton_events(void* const* events) {
+  t_newton_events_set = events != nullptr;
+  for (int i = 0; i < 4; ++i) t_newton_events[i] = events ? static_cast<cudaEvent_t>(events[i]) : nullptr;
+}
+
+static cudaError_t mark(int i, cudaStream_t stream) {
+  return t_newton_events_set ? cudaEventRecord(t_newton_events[i], stream) : cudaSuccess;
+}
+
+cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
+  const int cl = dual_cluster_size(imax(batch, args.concurrent), args.m);
+  const bool two = cl == 2;
+  cudaError_t e = mark(0, stream);
+  if (e != cudaSuccess) return e;
+  if (!(args.fp32_newton && args.approx_basis && dual32_supported(args.m, cl))) {
+    DualArgs a = args;
+    a.phase = 0;
+    if ((e = mark(1, stream)) != cudaSuccess || (e = mark(2, stream)) != cudaSuccess) return e;
+    e = launch_dual_phase(a, batch, two, stream);
+    return e == cudaSuccess ? mark(3, stream) : e;
+  }
+  // split form: basis set-up (FP64), early Newton steps (FP32), last steps and exit (FP64)
+  DualArgs a = args;
+  a.phase = 1;
+  e = launch_dual_phase(a, batch, two, stream);
+  if (e == cudaSuccess) e = mark(1, stream);
+  if (e != cudaSuccess) return e;
+  Dual32Args b{};
+  b.m = args.m;
+  b.max_newton = args.max_newton;
+  b.max_cg = args.max_cg;
+  b.max_backtrack = args.max_backtrack;
+  b.switch_tol = kFp32SwitchTol;
+  b.work = args.work;
+  b.scale = args.scale;
+  b.eig_status = args.eig_status;
+  b.adaptive = args.adaptive_precond;
+  e = launch_dual32(b, batch, cl, stream);
+  if (e == cudaSuccess) e = mark(2, stream);
+  if (e != cudaSuccess) return e;
+  a.phase = 2;
+  e = launch_dual_phase(a, batch, two, stream);
+  return e == cudaSuccess ? mark(3, stream) : e;
 }
 
 // ---------------------------------------------------------------- adjoint (implicit gradient)

@@ -9,8 +9,9 @@
 
 namespace ssn {
 
-// Number of m x m FP64 matrices of per-instance dual workspace.
-constexpr int kDualMats = 22;
+// Number of m x m FP64 matrices of per-instance dual workspace (the last one holds
+// small per-instance data: the FP32 phase's Newton updates and counters).
+constexpr int kDualMats = 23;
 
 // SM count of the current device, cached per device index (148 on B200; 148 if
 // the query fails).  Safe to call from several host threads.
@@ -34,7 +35,8 @@ struct DualArgs {
   double* Q;               // [B,m,m] out
   int64_t* iterations;     // [B] out
   int32_t* status;         // [B] out
-  int32_t* counters;       // [B,4] out: newton steps, hvps, trials, fallbacks (may be null)
+  int32_t* counters;       // [B,8] out (may be null): newton steps, hvps, trials, fallbacks of the
+                           // FP64 iteration, then of the FP32 phase (zero when it does not run)
   // Full rotated Gram: the kernel works with V^T (Cr/s) V in the sandwich
   // instead of assuming it is exactly diag(lambda), and takes lambda from its
   // diagonal.  Needed when the vectors only roughly diagonalise Cr/s (split
@@ -54,7 +56,28 @@ struct DualArgs {
   // Instances whose Newton kernels share the GPU at the same time (0: this batch
   // alone).  A 2-CTA cluster per instance pays only while SMs would otherwise idle.
   int concurrent;
+  // Split form: run the early Newton steps in FP32 (dual32_kernel) where the FP32
+  // state fits on chip, then the FP64 iteration warm-started from its omega.
+  int fp32_newton;
+  // dual_kernel phase: 0 the whole solve; 1 the basis set-up only (rotated Gram into
+  // the workspace); 2 the Newton iteration and exit after a phase-1 launch, started
+  // from the FP32 phase's omega when it took at least one Newton update.
+  int phase;
 };
+
+// The FP32 early Newton phase of the split form (ssn_dual32.cu).
+struct Dual32Args {
+  int m;
+  int max_newton, max_cg, max_backtrack;
+  double switch_tol;       // hand over to the FP64 iteration once the FP32 residual is below this
+  double* work;            // [B, kDualMats, m, m]: the phase-1 set-up in, omega and counters out
+  const double* scale;     // [B]
+  const int32_t* eig_status;  // [B] (may be null)
+  int adaptive;            // the Hessian-diagonal preconditioner for the CG steps
+};
+bool dual32_supported(int m, int cluster);
+cudaError_t launch_dual32(const Dual32Args& args, int batch, int cluster, cudaStream_t stream);
+int dual_cluster_size(int batch, int m);
 
 // Adjoint of the solve (implicit gradient), one CTA per instance.
 constexpr int kAdjointMats = 10;
@@ -94,6 +117,8 @@ cudaError_t launch_eigh_approx(const double* Cr, double* values, double* vectors
                                int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
                                int max_sweeps, bool fp32, float skip_corr, cudaStream_t stream);
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
+// Measurement hook behind ssn_set_newton_events (per host thread; null clears).
+void set_newton_events(void* const* events);
 // The whole uniform-batch solve (the body of ssn_solve) on one stream; `concurrent` as in DualArgs.
 int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch,
                 int n, int m, void* workspace, const ssn_options* opt, cudaStream_t stream, int concurrent);

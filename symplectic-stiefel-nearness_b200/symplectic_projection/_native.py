@@ -42,6 +42,7 @@ PROTOTYPES = {
     "ssn_dual": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
     "ssn_newton_workspace_bytes": (_SZ, [_I, _I]),
     "ssn_newton": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _SZ, _P, _P]),
+    "ssn_set_newton_events": (_I, [_P]),
     "ssn_probe_fp64_mma": (_I, [_P, _I, _P, _P]),
     "ssn_probe_s8_mma": (_I, [_P, _P, _P, _I, _I, _P, _P]),
     "ssn_inner_products": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
@@ -65,7 +66,8 @@ class Options(ctypes.Structure):
     _fields_ = [("max_newton", ctypes.c_int), ("max_cg", ctypes.c_int),
                 ("max_backtrack", ctypes.c_int), ("feas_tol", ctypes.c_double),
                 ("precision", ctypes.c_int), ("eig_sweeps", ctypes.c_int),
-                ("preconditioner", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+                ("preconditioner", ctypes.c_int), ("fp32_newton", ctypes.c_int),
+                ("reserved", ctypes.c_int * 4)]
 
 
 # ssn_options.precision / .preconditioner values (include/ssn.h)
@@ -94,7 +96,8 @@ def load() -> ctypes.CDLL:
 
 
 def options(max_newton=100, max_cg=150, max_backtrack=40, feas_tol=1e-8, precision="fp64",
-            eig_sweeps=0, preconditioner="eigenbasis") -> Options:
+            eig_sweeps=0, preconditioner="eigenbasis", fp32_newton=True) -> Options:
+    """ssn_options; fp32_newton (split form only): early Newton steps in FP32 (default) or all FP64."""
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     if preconditioner not in PRECONDITIONERS:
@@ -104,6 +107,7 @@ def options(max_newton=100, max_cg=150, max_backtrack=40, feas_tol=1e-8, precisi
     opt.max_newton, opt.max_cg, opt.max_backtrack, opt.feas_tol = max_newton, max_cg, max_backtrack, feas_tol
     opt.precision, opt.eig_sweeps = PRECISIONS[precision], eig_sweeps
     opt.preconditioner = PRECONDITIONERS[preconditioner]
+    opt.fp32_newton = 0 if fp32_newton else -1
     return opt
 
 

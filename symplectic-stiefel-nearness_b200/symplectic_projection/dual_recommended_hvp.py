@@ -64,7 +64,7 @@ def _pinned_like(T: torch.Tensor) -> torch.Tensor:
 def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
              max_backtrack: int = MAX_BACKTRACK, feas_tol: float = FEAS_TOL,
              precision: str = "fp64", eig_sweeps: int = 0, preconditioner: str = "eigenbasis",
-             raise_on_failure: bool = False) -> SolveResult:
+             fp32_newton: bool = True, raise_on_failure: bool = False) -> SolveResult:
     """Device-resident solve with per-instance status.  T must be a CUDA tensor.
 
     precision="fp64" is the plain FP64 form (the reference's iterates);
@@ -74,6 +74,9 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
     preconditioner="eigenbasis" (default) is the reference's; "adaptive" uses
     the Hessian diagonal at the current omega, which keeps ill-conditioned
     targets converging where the reference's CG saturates.
+    fp32_newton (split form): run the early Newton steps in FP32 where their
+    state fits on chip (m <= 96), the last step(s) and the convergence test in
+    FP64; False keeps every Newton step in FP64.
     """
     batch, n, m = _check_target(T)
     dev = N.require_cuda_f64(T)
@@ -87,7 +90,8 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
     lib = N.load()
     nbytes = lib.ssn_workspace_bytes(batch, n, m)
     ws = workspace(dev, nbytes)
-    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps, preconditioner)
+    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps, preconditioner,
+                    fp32_newton)
     N.check(lib.ssn_solve(T.data_ptr(), X.data_ptr(), omega.data_ptr(), iterations.data_ptr(),
                           status.data_ptr(), batch, n, m, ws.data_ptr(), nbytes,
                           N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_solve")
@@ -100,7 +104,7 @@ def solve_ex(T: torch.Tensor, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX
 def solve_ragged(targets, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
                  max_backtrack: int = MAX_BACKTRACK, feas_tol: float = FEAS_TOL,
                  precision: str = "fp64", eig_sweeps: int = 0, preconditioner: str = "eigenbasis",
-                 raise_on_failure: bool = True):
+                 fp32_newton: bool = True, raise_on_failure: bool = True):
     """Solve targets of different shapes in one call (ssn_solve_ragged).
 
     ``targets`` is a sequence of float64 [2n_i, 2k_i] tensors, all on the host or all
@@ -149,7 +153,8 @@ def solve_ragged(targets, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
     lib = N.load()
     nbytes = lib.ssn_ragged_workspace_bytes(count, n_arr, m_arr)
     ws = workspace(dev, nbytes)
-    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps, preconditioner)
+    opt = N.options(max_newton, max_cg, max_backtrack, feas_tol, precision, eig_sweeps, preconditioner,
+                    fp32_newton)
     N.check(lib.ssn_solve_ragged(flat.data_ptr(), X.data_ptr(), omega.data_ptr(), iterations.data_ptr(),
                                  status.data_ptr(), count, n_arr, m_arr, t_arr, w_arr, ws.data_ptr(), nbytes,
                                  N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_solve_ragged")
@@ -364,7 +369,7 @@ def dual_batch(Cr, Ci, final=None, **options):
     opt = N.options(options.get("max_newton", MAX_NEWTON), options.get("max_cg", MAX_CG),
                     options.get("max_backtrack", MAX_BACKTRACK), options.get("feas_tol", FEAS_TOL),
                     options.get("precision", "fp64"), options.get("eig_sweeps", 0),
-                    options.get("preconditioner", "eigenbasis"))
+                    options.get("preconditioner", "eigenbasis"), options.get("fp32_newton", True))
     N.check(lib.ssn_dual(Cr.data_ptr(), Ci.data_ptr(), omega.data_ptr(), P.data_ptr(), Q.data_ptr(),
                          iterations.data_ptr(), status.data_ptr(), batch, m, ws.data_ptr(), nbytes,
                          N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_dual")
