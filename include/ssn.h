@@ -205,6 +205,23 @@ int ssn_gram_noalloc(const double* A, const double* D, int64_t ab_stride, double
                      int batch, int rows, int m, ssn_stream_t stream);
 
 /*
+ * Cross Gram of two tall-skinny pairs G = [Ga; Gd] and T = [A; D]:
+ *   Mr = Ga^T A + Gd^T D,   Mi = Ga^T D - Gd^T A   (M = G^H b style product of
+ * the complex views g = Ga + i Gd, b = A + i D: M = conj(g)^T b).
+ * Ga, Gd are [batch, rows, m] with batch stride g_stride; A, D with ab_stride;
+ * Mr, Mi are [batch, m, m] contiguous (overwritten).  FP64 tensor-core (DMMA)
+ * products, row-split with a fixed-order sum of the split partials.  The
+ * reference computes these contractions with torch matmuls in its acceptance
+ * test (experiment.py:105-137: the tangent projection (J X)^T E of
+ * baselines/geometry.py:22-40) and in the adjoint's right-hand side.  Needs
+ * ssn_cross_gram_workspace_bytes bytes.
+ */
+size_t ssn_cross_gram_workspace_bytes(int batch, int rows, int m);
+int ssn_cross_gram(const double* Ga, const double* Gd, int64_t g_stride, const double* A,
+                   const double* D, int64_t ab_stride, double* Mr, double* Mi, int batch, int rows,
+                   int m, void* workspace, size_t workspace_bytes, ssn_stream_t stream);
+
+/*
  * Recovery products:  Ur = A P^T + D Q^T,  Ui = D P^T - A Q^T.
  * A, D, Ur, Ui are [batch, rows, m] with batch strides ab_stride / u_stride;
  * P, Q are [batch, m, m] contiguous.  Replaces recover_block
@@ -336,6 +353,11 @@ int ssn_inverse_from_cholesky(const double* L, double* P, int batch, int m, ssn_
  * pivot is positive, else the 1-based failing pivot), the device equivalent of
  * torch.linalg.cholesky_ex + construct_inverse (dual_recommended_hvp.py:173-176). */
 int ssn_spd_inverse(const double* K, double* P, int32_t* info, int batch, int m, ssn_stream_t stream);
+/* L = chol(I + omega omega), lower triangular, for skew omega [batch, m, m]
+ * (dual_recommended_hvp.py:63 and :173, torch.linalg.cholesky(I + omega @ omega);
+ * dual_batch returns this L).  info[b] = 0, or the 1-based order of the first
+ * leading minor that is not positive definite (L's columns from there are 0). */
+int ssn_cholesky_k(const double* omega, double* L, int32_t* info, int batch, int m, ssn_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -318,6 +318,24 @@ int ssn_gram(const double* A, const double* D, int64_t ab_stride, double* Cr, do
   return cuda_status(launch_gram(A, D, ab_stride, Cr, Ci, batch, rows, m, static_cast<double*>(workspace), st));
 }
 
+size_t ssn_cross_gram_workspace_bytes(int batch, int rows, int m) {
+  if (!shape_ok(batch, m) || rows < 1) return 0;
+  return gram_fp64_bytes(batch, rows, m);
+}
+
+int ssn_cross_gram(const double* Ga, const double* Gd, int64_t g_stride, const double* A, const double* D,
+                   int64_t ab_stride, double* Mr, double* Mi, int batch, int rows, int m, void* workspace,
+                   size_t workspace_bytes, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || rows < 1 || !Ga || !Gd || !A || !D || !Mr || !Mi ||
+      g_stride < (int64_t)rows * m || ab_stride < (int64_t)rows * m || (g_stride % 2) != 0 ||
+      (ab_stride % 2) != 0 || !aligned16(Ga) || !aligned16(Gd) || !aligned16(A) || !aligned16(D))
+    return SSN_ERR_INVALID_ARGUMENT;
+  if (!workspace || workspace_bytes < ssn_cross_gram_workspace_bytes(batch, rows, m) || !aligned16(workspace))
+    return SSN_ERR_WORKSPACE;
+  return cuda_status(launch_cross_gram(Ga, Gd, g_stride, A, D, ab_stride, Mr, Mi, batch, rows, m,
+                                       static_cast<double*>(workspace), reinterpret_cast<cudaStream_t>(stream)));
+}
+
 size_t ssn_recover_workspace_bytes(int batch, int rows, int m) {
   if (!shape_ok(batch, m) || rows < 1) return 0;
   return ozaki_recover_workspace_bytes(batch, rows, m);
@@ -518,6 +536,11 @@ int ssn_inverse_from_cholesky(const double* L, double* P, int batch, int m, ssn_
 int ssn_spd_inverse(const double* K, double* P, int32_t* info, int batch, int m, ssn_stream_t stream) {
   if (!shape_ok(batch, m) || !K || !P || !info) return SSN_ERR_INVALID_ARGUMENT;
   return cuda_status(launch_spd_inverse(K, P, info, batch, m, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int ssn_cholesky_k(const double* omega, double* L, int32_t* info, int batch, int m, ssn_stream_t stream) {
+  if (!shape_ok(batch, m) || !omega || !L || !info) return SSN_ERR_INVALID_ARGUMENT;
+  return cuda_status(launch_cholesky_k(omega, L, info, batch, m, reinterpret_cast<cudaStream_t>(stream)));
 }
 
 }  // extern "C"

@@ -168,6 +168,67 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// L = chol(I + omega omega) for a skew omega (dual_recommended_hvp.py:63 and :173,
+// torch.linalg.cholesky(I + omega @ omega)).  One CTA per instance: the lower
+// triangle of K = I + omega omega is formed from omega staged in shared memory
+// (through L's own storage, so one m x m array of shared memory suffices), then
+// factored column by column (right-looking).  info = 0, or the order of the
+// first leading minor that is not positive definite (L's columns from there
+// are 0).
+__global__ void __launch_bounds__(kThreads, 1)
+    cholesky_k_kernel(const double* omega, double* L, int32_t* info, int m) {
+  extern __shared__ __align__(16) double smem[];
+  const int ld = m + 1;
+  double* K = smem;
+  __shared__ int bad;
+  const size_t off = (size_t)blockIdx.x * m * m;
+  for (int e = threadIdx.x; e < m * m; e += kThreads) {
+    const int i = e / m, j = e - i * m;
+    K[i * ld + j] = omega[off + e];
+  }
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int e = threadIdx.x; e < m * m; e += kThreads) {
+    const int i = e / m, j = e - i * m;
+    if (j > i) continue;
+    double s = (i == j) ? 1.0 : 0.0;
+    for (int k = 0; k < m; ++k) s = fma(K[i * ld + k], K[k * ld + j], s);
+    L[off + e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < m * m; e += kThreads) {
+    const int i = e / m, j = e - i * m;
+    if (j <= i) K[i * ld + j] = L[off + e];
+  }
+  __syncthreads();
+  for (int j = 0; j < m; ++j) {
+    const double d = K[j * ld + j];
+    if (!(d > 0.0) || !isfinite(d)) {
+      if (threadIdx.x == 0) bad = j + 1;
+      break;
+    }
+    const double r = sqrt(d);
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < m; i += kThreads) K[i * ld + j] /= r;
+    if (threadIdx.x == 0) K[j * ld + j] = r;
+    __syncthreads();
+    // trailing update of the lower triangle: K[i][l] -= L[i][j] L[l][j], j < l <= i
+    const int t = m - j - 1;
+    for (int e = threadIdx.x; e < t * t; e += kThreads) {
+      const int i = j + 1 + e / t, l = j + 1 + e % t;
+      if (l <= i) K[i * ld + l] = fma(-K[i * ld + j], K[l * ld + j], K[i * ld + l]);
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  const int fail = bad;
+  for (int e = threadIdx.x; e < m * m; e += kThreads) {
+    const int i = e / m, j = e - i * m;
+    L[off + e] = (j <= i && (fail == 0 || j < fail - 1)) ? K[i * ld + j] : 0.0;
+  }
+  if (threadIdx.x == 0) info[blockIdx.x] = fail;
+}
+
 #define SSN_MB_DISPATCH(KERNEL, SMEM, ...)                                              \
   do {                                                                                  \
     cudaError_t e_ = cudaSuccess;                                                       \
@@ -234,6 +295,15 @@ cudaError_t launch_inverse_from_cholesky(const double* L, double* P, int batch, 
   cudaError_t err = prep(inverse_from_cholesky_kernel, smem);
   if (err != cudaSuccess) return err;
   inverse_from_cholesky_kernel<<<batch, kThreads, smem, stream>>>(L, P, m);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cholesky_k(const double* omega, double* L, int32_t* info, int batch, int m,
+                              cudaStream_t stream) {
+  const size_t smem = sizeof(double) * (size_t)m * (m + 1);
+  cudaError_t err = prep(cholesky_k_kernel, smem);
+  if (err != cudaSuccess) return err;
+  cholesky_k_kernel<<<batch, kThreads, smem, stream>>>(omega, L, info, m);
   return cudaGetLastError();
 }
 

@@ -180,5 +180,7 @@ cudaError_t launch_spd_inverse(const double* K, double* P, int32_t* info, int ba
                                cudaStream_t stream);
 cudaError_t launch_inverse_from_cholesky(const double* L, double* P, int batch, int m,
                                          cudaStream_t stream);
+cudaError_t launch_cholesky_k(const double* omega, double* L, int32_t* info, int batch, int m,
+                              cudaStream_t stream);
 
 }  // namespace ssn

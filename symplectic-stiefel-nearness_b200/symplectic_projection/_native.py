@@ -34,6 +34,8 @@ PROTOTYPES = {
     "ssn_gram": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_gram_noalloc_scratch_bytes": (_SZ, []),
     "ssn_gram_noalloc": (_I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P]),
+    "ssn_cross_gram_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "ssn_cross_gram": (_I, [_P, _P, _I64, _P, _P, _I64, _P, _P, _I, _I, _I, _P, _SZ, _P]),
     "ssn_recover_workspace_bytes": (_SZ, [_I, _I, _I]),
     "ssn_recover": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I, _I, _P, _SZ, _P, _P]),
     "ssn_eigh_workspace_bytes": (_SZ, [_I, _I]),
@@ -54,6 +56,7 @@ PROTOTYPES = {
     "ssn_cg_next": (_I, [_P, _P, _P, _P, _P, _I, _I, _P]),
     "ssn_inverse_from_cholesky": (_I, [_P, _P, _I, _I, _P]),
     "ssn_spd_inverse": (_I, [_P, _P, _P, _I, _I, _P]),
+    "ssn_cholesky_k": (_I, [_P, _P, _P, _I, _I, _P]),
 }
 
 SSN_OK = 0
@@ -123,6 +126,25 @@ def ptr(t: torch.Tensor | None) -> int | None:
 
 def stream_handle(device: torch.device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
+
+
+def row_halves(A: torch.Tensor, D: torch.Tensor):
+    """(A, D, batch stride) for a pair of [batch, rows, m] operands of one kernel call.
+
+    The C ABI takes both halves with one batch stride and densely packed rows, as
+    the two halves T[:, :n] and T[:, n:] of a target batch are; such views pass
+    without a copy.  Other layouts are made contiguous.
+    """
+    batch, rows, m = A.shape
+
+    def packed(x):
+        return x.stride(2) == 1 and x.stride(1) == m and x.data_ptr() % 16 == 0
+
+    if packed(A) and packed(D):
+        stride = rows * m if batch == 1 else A.stride(0)
+        if (batch == 1 or D.stride(0) == stride) and stride >= rows * m and stride % 2 == 0:
+            return A, D, stride
+    return A.contiguous(), D.contiguous(), rows * m
 
 
 def require_cuda_f64(*tensors: torch.Tensor) -> torch.device:

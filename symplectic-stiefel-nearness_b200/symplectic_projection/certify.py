@@ -11,9 +11,12 @@ checker ``inspect_output`` (src/symplectic_projection/experiment.py:105-137):
           C = b^H b with b = T_top + i T_bottom (the same value as the
           reference's ||L^-1 b^H||^2, written through the Gram matrix).
 
-Gram products, eigendecompositions and SPD inverses use this package's
-kernels; the remaining small batched products and norms use torch on the GPU.
-It runs outside any timed region: it is the batch's self-certificate.
+Every tall-skinny contraction runs on this package's FP64 tensor-core kernels:
+the Grams of X and T (ssn_gram), the cross product (J X)^T E (ssn_cross_gram)
+and the tangent correction [-Yb M; Yt M] (ssn_recover with P = 0, Q = M); so do
+the eigendecomposition and the SPD inverse.  The m x m products of the
+multiplier's eigenbasis transform and the element-wise norms use torch on the
+GPU.  It runs outside any timed region: it is the batch's self-certificate.
 """
 from __future__ import annotations
 
@@ -23,7 +26,8 @@ import torch
 
 from .cholesky_inverse_kernel import spd_inverse
 from .dual_recommended_hvp import eigh_scaled
-from .gram_triangle_reflect import gram
+from .gram_triangle_reflect import cross_gram, gram
+from .recovery_fused import recover_block
 
 THRESHOLDS = {"feasibility": 1e-8, "stationarity": 1e-9, "delta": 1e-8}
 
@@ -52,15 +56,16 @@ def certify(T: torch.Tensor, X: torch.Tensor) -> dict:
     values, vectors, scale, _ = eigh_scaled(CrY)
     lam = values * scale[:, None]
     den = lam[:, :, None] + lam[:, None, :]
-    coupling = Yb.mT @ Et - Yt.mT @ Eb                 # (J X)^T E
-    rhs = coupling - coupling.mT
+    # (J X)^T E = Yb^T Et - Yt^T Eb = -Mi of the cross Gram of (X, E)
+    _, Mi = cross_gram(Yt, Yb, Et, Eb)
+    rhs = Mi.mT - Mi
     rotated = vectors.mT @ rhs @ vectors
     mult = vectors @ (rotated / den) @ vectors.mT
     mult = (mult - mult.mT) / 2
-    grad_t = Et - Yb @ mult
-    grad_b = Eb + Yt @ mult
-    gnorm = torch.sqrt(torch.linalg.vector_norm(grad_t, dim=(-2, -1)) ** 2 +
-                       torch.linalg.vector_norm(grad_b, dim=(-2, -1)) ** 2)
+    # [Et - Yb mult; Eb + Yt mult] = E + recovery of (Yt, Yb) with P = 0, Q = mult (skew)
+    Ut, Ub = recover_block(Yt, Yb, torch.zeros_like(mult), mult)
+    grad = torch.cat((Et + Ut, Eb + Ub), dim=1)
+    gnorm = torch.linalg.vector_norm(grad, dim=(-2, -1))
     tnorm = torch.linalg.vector_norm(T, dim=(-2, -1))
     stat = gnorm / (2 * tnorm.clamp_min(1.0))
 

@@ -34,3 +34,20 @@ def spd_inverse(K):
     N.check(N.load().ssn_spd_inverse(K.data_ptr(), P.data_ptr(), info.data_ptr(), batch, m,
                                      N.stream_handle(dev)), "ssn_spd_inverse")
     return P, info
+
+
+@torch.no_grad()
+def cholesky_k(omega):
+    """(L, info): L = chol(I + omega omega) for skew omega [batch, m, m] (dual_recommended_hvp.py:63).
+
+    info[b] == 0 iff I + omega omega is positive definite (else the 1-based
+    order of the first leading minor that is not).
+    """
+    dev = N.require_cuda_f64(omega)
+    batch, m, _ = omega.shape
+    omega = omega.contiguous()
+    L = torch.empty_like(omega)
+    info = torch.empty(batch, dtype=torch.int32, device=dev)
+    N.check(N.load().ssn_cholesky_k(omega.data_ptr(), L.data_ptr(), info.data_ptr(), batch, m,
+                                    N.stream_handle(dev)), "ssn_cholesky_k")
+    return L, info

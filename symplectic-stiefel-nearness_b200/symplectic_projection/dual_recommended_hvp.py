@@ -18,6 +18,7 @@ import torch
 
 from . import _native as N
 from ._workspace import workspace
+from .cholesky_inverse_kernel import cholesky_k
 
 # dual_recommended_hvp.py:13-19
 ROW_CHUNK = 1024
@@ -353,7 +354,7 @@ def dual_batch(Cr, Ci, final=None, **options):
 
     If ``final`` is a list it receives (P, Q), the cached inverse parts in the
     original basis, like the reference.  L = chol(I + omega omega) is formed
-    with torch.linalg.cholesky only to keep the reference's return shape; the
+    by this package's Cholesky kernel to keep the reference's return value; the
     solve path does not use it.
     """
     dev = N.require_cuda_f64(Cr, Ci)
@@ -376,8 +377,9 @@ def dual_batch(Cr, Ci, final=None, **options):
     raise_for_status(status)
     if final is not None:
         final[:] = (P, Q)
-    eye = torch.eye(m, dtype=torch.float64, device=dev)
-    L = torch.linalg.cholesky(eye + omega @ omega)
+    L, info = cholesky_k(omega)
+    if bool((info != 0).any()):
+        raise torch.linalg.LinAlgError("dual_batch: I + omega omega is not positive definite")
     return omega, L, iterations
 
 

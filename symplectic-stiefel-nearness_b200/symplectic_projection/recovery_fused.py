@@ -20,13 +20,15 @@ def recover_block(A, D, P, Q, precision="fp64"):
     batch, rows, m = A.shape
     if D.shape != A.shape or P.shape != (batch, m, m) or Q.shape != (batch, m, m):
         raise ValueError("shape mismatch")
-    A, D, P, Q = (x.contiguous() for x in (A, D, P, Q))
-    Ur, Ui = torch.empty_like(A), torch.empty_like(A)
+    A, D, ab_stride = N.row_halves(A, D)
+    P, Q = P.contiguous(), Q.contiguous()
+    Ur = torch.empty(batch, rows, m, dtype=torch.float64, device=dev)
+    Ui = torch.empty_like(Ur)
     lib = N.load()
     nbytes = lib.ssn_recover_workspace_bytes(batch, rows, m)
     ws = workspace(dev, nbytes)
     opt = N.options(precision=precision)
-    N.check(lib.ssn_recover(A.data_ptr(), D.data_ptr(), rows * m, P.data_ptr(), Q.data_ptr(),
+    N.check(lib.ssn_recover(A.data_ptr(), D.data_ptr(), ab_stride, P.data_ptr(), Q.data_ptr(),
                             Ur.data_ptr(), Ui.data_ptr(), rows * m, batch, rows, m, ws.data_ptr(), nbytes,
                             N.ctypes.byref(opt), N.stream_handle(dev)), "ssn_recover")
     return Ur, Ui

@@ -165,3 +165,84 @@ def test_recover_block(sp, m, rows):
     Ur, Ui = sp.recovery_fused.recover_block(A.cuda(), D.cuda(), P.cuda(), Q.cuda())
     wr, wi = O.recover(A, D, P, Q)
     assert rel(Ur, wr) < 1e-13 and rel(Ui, wi) < 1e-13
+
+
+@pytest.mark.parametrize("m,rows", [(2, 5), (24, 100), (96, 1000), (128, 129), (96, 4096)])
+def test_cross_gram(sp, m, rows):
+    g = torch.Generator().manual_seed(80 + m)
+    Ga, Gd, A, D = (torch.randn(3, rows, m, dtype=torch.float64, generator=g) for _ in range(4))
+    Mr, Mi = sp.gram_triangle_reflect.cross_gram(Ga.cuda(), Gd.cuda(), A.cuda(), D.cuda())
+    assert rel(Mr, Ga.mT @ A + Gd.mT @ D) < 1e-13
+    assert rel(Mi, Ga.mT @ D - Gd.mT @ A) < 1e-13
+
+
+def test_products_take_the_halves_of_a_stacked_batch_without_a_copy(sp):
+    # T[:, :n] and T[:, n:] share one batch stride: the entry points read them in place
+    T, _ = O.make_inputs(300, 20, 4, 3)
+    Td = T.cuda()
+    n = 300
+    A, D = Td[:, :n], Td[:, n:]
+    from symplectic_projection import _native as N
+    a, d, stride = N.row_halves(A, D)
+    assert a.data_ptr() == A.data_ptr() and d.data_ptr() == D.data_ptr() and stride == 2 * n * 40
+    Cr, Ci = sp.gram_triangle_reflect.gram(A, D)
+    wr, wi = O.gram(T)
+    assert rel(Cr, wr) < 1e-13 and rel(Ci, wi) < 1e-13
+    P, Q = rand(3, 40, 72, sym=True), rand(3, 40, 73, skew=True)
+    Ur, Ui = sp.recovery_fused.recover_block(A, D, P.cuda(), Q.cuda())
+    vr, vi = O.recover(T[:, :n], T[:, n:], P, Q)
+    assert rel(Ur, vr) < 1e-13 and rel(Ui, vi) < 1e-13
+    Mr, Mi = sp.gram_triangle_reflect.cross_gram(A, D, D, A)
+    assert rel(Mr, T[:, :n].mT @ T[:, n:] + T[:, n:].mT @ T[:, :n]) < 1e-13
+
+
+@pytest.mark.parametrize("m", [2, 8, 24, 96, 128])
+def test_cholesky_k_and_pd_flag(sp, m):
+    W = rand(4, m, 90, skew=True)
+    W = W / torch.linalg.matrix_norm(W, ord=2)[:, None, None]
+    W[0] *= 0.5
+    W[1] *= 0.99
+    W[2] *= 1.5            # I + W W not positive definite
+    W[3] *= 0.0
+    K = torch.eye(m, dtype=torch.float64) + W @ W
+    L, info = sp.cholesky_inverse_kernel.cholesky_k(W.cuda())
+    ref, ref_info = torch.linalg.cholesky_ex(K)
+    assert info.cpu().ne(0).tolist() == ref_info.ne(0).tolist()
+    ok = ref_info == 0
+    L = L.cpu()
+    assert torch.equal(L[ok], L[ok].tril())
+    assert rel(L[ok], ref[ok]) < 1e-12
+    if m > 2:
+        bad = int(info[2])
+        assert 1 <= bad <= m and bool((L[2][:, bad - 1:] == 0).all())
+
+
+def test_dual_batch_returns_the_cholesky_factor(sp):
+    from symplectic_projection.dual_recommended_hvp import dual_batch
+    T, _ = O.make_inputs(64, 8, 6, 3)
+    Cr, Ci = O.gram(T)
+    final = []
+    omega, L, it = dual_batch(Cr.cuda(), Ci.cuda(), final)
+    m = omega.shape[-1]
+    K = torch.eye(m, dtype=torch.float64) + omega.cpu() @ omega.cpu()
+    assert rel(L, torch.linalg.cholesky(K)) < 1e-12
+
+
+@pytest.mark.parametrize("n,k,B", [(64, 8, 4), (2048, 48, 3)])
+def test_certify_matches_the_oracle_acceptance_test(sp, n, k, B):
+    from symplectic_projection.certify import certify
+    T, _ = O.make_inputs(n, k, 7, B)
+    X, _, _ = O.solve(T)
+    X = X.clone()
+    X[1] += 1e-6 * torch.randn(X[1].shape, dtype=torch.float64, generator=torch.Generator().manual_seed(1))
+    cert = certify(T.cuda(), X.cuda())
+    recs = O.inspect_output(T, X)
+    for key in ("feasibility", "stationarity"):
+        got = cert[key].cpu()
+        want = torch.tensor([r[key] for r in recs], dtype=torch.float64)
+        assert torch.allclose(got, want, rtol=1e-6, atol=1e-15), key
+    delta = cert["delta"].cpu()
+    want = torch.tensor([r["delta"] for r in recs], dtype=torch.float64)
+    assert torch.allclose(delta, want, rtol=1e-3, atol=1e-12)
+    assert cert["passed"].cpu().tolist() == [O.passes(r) for r in recs]
+    assert cert["passed"].cpu().tolist()[1] is False
