@@ -73,6 +73,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-side-legs", action="store_true",
+                   help="skip the library peak GEMMs and the reference GPU leg (small profiling runs)")
     p.add_argument("--precision", choices=["split", "fp64", "both"], default="both",
                    help="form timed for `value` (split when both; the FP64 form is then reported beside it)")
     p.add_argument("--eig-sweeps", type=int, default=0, help="split form: Jacobi sweeps (0 = library default)")
@@ -350,7 +352,9 @@ def run_ours(args):
         e1.synchronize()
         peak = max(peak, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
     hbm_gbs, hbm_src = hbm_peak()
-    peaks = library_peaks(torch, dev, stream)
+    peaks = ({"fp64": float("nan"), "fp32": float("nan"), "int8": float("nan"),
+              "source": "not measured (--no-side-legs)"} if args.no_side_legs
+             else library_peaks(torch, dev, stream))
     peaks["fp64_probe"] = peak
 
     solve_bytes = lib.ssn_workspace_bytes(B, n, m)
@@ -603,7 +607,7 @@ def run_ours(args):
             "peaks": dict(peaks), "phases": phases_out}
     if compare:
         line.update(compare)
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_side_legs:
         line["reference_gpu"] = reference_gpu(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, args.cpu_seconds)

@@ -32,11 +32,15 @@
 //    d, r, p (and of the adaptive preconditioner), and computes exactly that
 //    tile (or its transpose, for column-split products) in every product, so
 //    the element-wise PCG work needs no shared-memory traffic.
-// Products are register-tiled FP32 SIMT outer products: for each k, one
-// 16-byte shared load of A's row segment and one of B's per operand, 16 FFMAs
-// per operand pair, with the next k's operands loaded while the current FFMAs
-// run.  Symmetric and antisymmetric operands are read through their
-// transposes (P^T = P, Q^T = -Q, ...), so every operand is a row segment.
+// Products run on the tensor cores (mma.sync m16n8k8 TF32): each warp computes
+// the 16 x 32 (or 32 x 16) block of the product that its 32 threads' 4 x 4
+// tiles make up, and hands the tiles out through a small per-warp staging area.
+// The products that set the iterate -- Q = -omega P, the sandwich and the trial
+// K -- use the 3xTF32 split (hi*hi + hi*lo + lo*hi, about 2^-21 relative per
+// term); the CG's HVPs and the line search's change, whose errors only perturb
+// the inexact Newton direction and the Armijo test, use one TF32 product.
+// Symmetric and antisymmetric operands are read through their transposes
+// (P^T = P, Q^T = -Q, ...), so every operand is a row segment.
 //
 // All decisions (convergence, CG stop, acceptance) follow reductions summed
 // in FP64 in a fixed order, identical in both CTAs of a cluster, so all
@@ -73,14 +77,15 @@ struct G32 {
   static constexpr int SS = YF;
   static constexpr int NRED = 5;              // values of the widest fused reduction
   // offsets in floats
+  static constexpr int STAGE = 384;           // floats per warp: tensor-core product tiles -> 4 x 4 tiles
   static constexpr int O_P = 0, O_Q = O_P + FULL, O_X = O_Q + FULL, O_Y = O_X + FULL, O_Z = O_Y + YF,
                        O_S = O_Z + OWNC, O_LAM = O_S + SS, O_PD = O_LAM + MP, O_SD = O_PD + MP,
-                       FLOATS = round_up(O_SD + MP, 4);
+                       O_ST = round_up(O_SD + MP, 4), FLOATS = O_ST + STAGE * WARPS;
   static constexpr size_t bytes() {
     return sizeof(float) * FLOATS + sizeof(double) * (NRED * WARPS + 4 * NRED) + 64;
   }
   static_assert(THREADS % 32 == 0 && TA % 4 == 0 && TB % 8 == 0, "tile grid");
-  static_assert(16 * LDF + 16 * MP <= OWNC, "the inverse's pivot panels fit the Z buffer");
+  static_assert(32 * LDF <= OWNC, "the inverse's pivot panels fit the Z buffer");
   static_assert(OWNR <= OWNC, "own rows of Si' fit the Z buffer");
 };
 
@@ -152,6 +157,155 @@ __device__ __forceinline__ void outer(const uint32_t (&A)[NA], int lda, int u, c
           }
         }
   }
+}
+
+// ---- the same products on the tensor cores: mma.sync m16n8k8 TF32 in the 3xTF32 form.
+// Each FP32 operand x is split as hi = tf32(x), lo = tf32(x - hi), and a product is
+// hi*hi + hi*lo + lo*hi with FP32 accumulation: about 2^-21 relative per product term
+// (the lo*lo term and the rounding of lo are below it), against 2^-24 for FFMA.
+__device__ __forceinline__ uint32_t lds1(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.b32 %0, [%1];\n" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void split_tf32(uint32_t x, uint32_t& hi, uint32_t& lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(hi) : "f"(__uint_as_float(x)));
+  const float r = __uint_as_float(x) - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(lo) : "f"(r));
+}
+__device__ __forceinline__ uint32_t to_tf32(uint32_t x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(__uint_as_float(x)));
+  return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// outer() on the tensor cores, for the kernel's thread layout: lane l of a warp owns the
+// 4 x 4 tile (u, v) with u = u0 + (l >> 3), v = v0 + (l & 7) (TR = false: a 16 x 32 warp
+// tile, one m16 x four n8 MMA tiles) or u = u0 + (l & 7), v = v0 + (l >> 3) (TR = true:
+// 32 x 16, two m16 x two n8).  The accumulator fragments go through the warp's STAGE
+// floats of shared memory (one half of the warp tile at a time) into the 4 x 4 tiles.
+// All 32 lanes of the warp call it together.
+template <int NA, int NB, int NOUT, uint32_t COEF, int K, bool TR, bool X3 = true>
+__device__ __forceinline__ void outer_tc(const uint32_t (&A)[NA], int lda, int u, const uint32_t (&B)[NB], int ldb,
+                                         int v, float* stage, float (&acc)[NOUT][4][4]) {
+  constexpr int MT = TR ? 2 : 1, NT = TR ? 2 : 4;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int lr = TR ? (lane & 7) : (lane >> 3), lc = TR ? (lane >> 3) : (lane & 7);
+  const uint32_t R0 = 4u * (uint32_t)(u - lr), C0 = 4u * (uint32_t)(v - lc);   // warp tile origin
+  float c[NOUT][MT * NT][4];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+    for (int q = 0; q < MT * NT; ++q)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) c[o][q][e] = 0.0f;
+#pragma unroll 1
+  for (int k = 0; k < K; k += 8) {
+#pragma unroll
+    for (int mi = 0; mi < MT; ++mi) {
+      // A fragments: a0 = (row g, k t), a1 = (g + 8, t), a2 = (g, t + 4), a3 = (g + 8, t + 4)
+      uint32_t ah[NA][4], al[NA][X3 ? 4 : 1];
+#pragma unroll
+      for (int ia = 0; ia < NA; ++ia) {
+        const uint32_t base = A[ia] + 4u * ((uint32_t)(k + t) * lda + R0 + 16u * mi + g);
+        const uint32_t x0 = lds1(base), x1 = lds1(base + 32u);
+        const uint32_t x2 = lds1(base + 16u * lda), x3 = lds1(base + 16u * lda + 32u);
+        if constexpr (X3) {
+          split_tf32(x0, ah[ia][0], al[ia][0]);
+          split_tf32(x1, ah[ia][1], al[ia][1]);
+          split_tf32(x2, ah[ia][2], al[ia][2]);
+          split_tf32(x3, ah[ia][3], al[ia][3]);
+        } else {
+          ah[ia][0] = to_tf32(x0);
+          ah[ia][1] = to_tf32(x1);
+          ah[ia][2] = to_tf32(x2);
+          ah[ia][3] = to_tf32(x3);
+        }
+      }
+#pragma unroll
+      for (int nj = 0; nj < NT; ++nj) {
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) {
+          // B fragment: b0 = (k t, column g), b1 = (k t + 4, g)
+          const uint32_t base = B[ib] + 4u * ((uint32_t)(k + t) * ldb + C0 + 8u * nj + g);
+          uint32_t bh0, bl0 = 0u, bh1, bl1 = 0u;
+          if constexpr (X3) {
+            split_tf32(lds1(base), bh0, bl0);
+            split_tf32(lds1(base + 16u * ldb), bh1, bl1);
+          } else {
+            bh0 = to_tf32(lds1(base));
+            bh1 = to_tf32(lds1(base + 16u * ldb));
+          }
+#pragma unroll
+          for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia) {
+              const int sg = coef_get(COEF, o, ia, ib);
+              if (sg == 0) continue;
+              const uint32_t f = sg == 2 ? 0x80000000u : 0u;   // negate the A operand
+              float (&cc)[4] = c[o][mi * NT + nj];
+              if constexpr (X3) {
+                mma_tf32(cc, al[ia][0] ^ f, al[ia][1] ^ f, al[ia][2] ^ f, al[ia][3] ^ f, bh0, bh1);
+                mma_tf32(cc, ah[ia][0] ^ f, ah[ia][1] ^ f, ah[ia][2] ^ f, ah[ia][3] ^ f, bl0, bl1);
+              }
+              mma_tf32(cc, ah[ia][0] ^ f, ah[ia][1] ^ f, ah[ia][2] ^ f, ah[ia][3] ^ f, bh0, bh1);
+            }
+        }
+      }
+    }
+  }
+  // fragments (row g / g + 8, columns 2 t, 2 t + 1 of each n8 tile) -> 4 x 4 tiles
+  constexpr int LD = TR ? 24 : 40;
+  float* st = stage + (threadIdx.x >> 5) * 384;
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      __syncwarp();
+      if constexpr (!TR) {
+        // half h: rows 8 h .. 8 h + 7 of the 16 x 32 tile
+#pragma unroll
+        for (int nj = 0; nj < NT; ++nj)
+          *reinterpret_cast<float2*>(st + g * LD + 8 * nj + 2 * t) =
+              make_float2(c[o][nj][2 * h], c[o][nj][2 * h + 1]);
+        __syncwarp();
+        // every lane reads (rows clamped into the half)
+        const bool mine = (lr >> 1) == h;
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+          const float4 w = ld4(st + ((4 * lr + x) & 7) * LD + 4 * lc);
+          // the first half is taken by every lane (so no earlier value of acc stays live),
+          // the second only by its owners
+          if (h == 0 || mine) { acc[o][x][0] = w.x; acc[o][x][1] = w.y; acc[o][x][2] = w.z; acc[o][x][3] = w.w; }
+        }
+      } else {
+        // half h: m16 tile h, rows 16 h .. 16 h + 15 of the 32 x 16 tile
+#pragma unroll
+        for (int nj = 0; nj < NT; ++nj) {
+          *reinterpret_cast<float2*>(st + g * LD + 8 * nj + 2 * t) =
+              make_float2(c[o][h * NT + nj][0], c[o][h * NT + nj][1]);
+          *reinterpret_cast<float2*>(st + (g + 8) * LD + 8 * nj + 2 * t) =
+              make_float2(c[o][h * NT + nj][2], c[o][h * NT + nj][3]);
+        }
+        __syncwarp();
+        const bool mine = (lr >> 2) == h;
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+          const float4 w = ld4(st + ((4 * lr + x) & 15) * LD + 4 * lc);
+          // the first half is taken by every lane (so no earlier value of acc stays live),
+          // the second only by its owners
+          if (h == 0 || mine) { acc[o][x][0] = w.x; acc[o][x][1] = w.y; acc[o][x][2] = w.z; acc[o][x][3] = w.w; }
+        }
+      }
+    }
+  __syncwarp();
 }
 
 // The CTAs of one instance: sync() is the phase barrier; sumv() sums N values over the
@@ -230,6 +384,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
   float* lam = sm + G::O_LAM;     // diagonal of the rotated Gram (1 on the padding)
   float* pdg = sm + G::O_PD;      // diag(P), diag(Sr): the adaptive preconditioner
   float* sdg = sm + G::O_SD;
+  float* stg = sm + G::O_ST;      // per-warp staging of the tensor-core product tiles
   double* red = reinterpret_cast<double*>(sm + G::FLOATS);
   double* xch = red + G::NRED * G::WARPS;
   int* flags = reinterpret_cast<int*>(xch + 4 * G::NRED);   // pivot-block outcome of the inverse
@@ -364,7 +519,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
         float q[1][4][4];
         const uint32_t A[1] = {saddr(Zb)};
         const uint32_t B[1] = {saddr(Pf)};
-        outer<1, 1, 1, coef_bit(0, 0, 0, 2), MP>(A, LDO, ta, B, LDF, tb, q);
+        outer_tc<1, 1, 1, coef_bit(0, 0, 0, 2), MP, false>(A, LDO, ta, B, LDF, tb, stg, q);
         put_rows_full(Qf, q[0]);
       }
       // the constant rotated Gram, staged for the sandwich
@@ -380,7 +535,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
         const uint32_t B[2] = {saddr(Yf), saddr(Ss)};
         constexpr uint32_t C = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1) | coef_bit(1, 0, 1, 1) |
                                coef_bit(1, 1, 0, 2);
-        outer<2, 2, 2, C, MP>(A, LDF, ta, B, LDF, tb, y);
+        outer_tc<2, 2, 2, C, MP, false>(A, LDF, ta, B, LDF, tb, stg, y);
       }
       __syncthreads();                      // the staged Gram is consumed
       put_rows_T(Yf, y[0]);
@@ -393,7 +548,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
         const uint32_t B[2] = {saddr(Pf), saddr(Qf)};
         constexpr uint32_t C = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 2) | coef_bit(1, 1, 0, 1) |
                                coef_bit(1, 0, 1, 1);
-        outer<2, 2, 2, C, MP>(A, LDO, ta, B, LDF, tb, y);
+        outer_tc<2, 2, 2, C, MP, false>(A, LDO, ta, B, LDF, tb, stg, y);
       }
       // Sr = sym(Sr'), Si = skew(Si') with the transposed entries from the CTA owning them:
       // this CTA's rows of Sr' in Xf, of Si' in Zb (own-row layout, leading dim LDF)
@@ -518,7 +673,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
           const uint32_t A[1] = {saddr(Xf)};
           const uint32_t B[2] = {saddr(Ss), saddr(Ss + G::OWNC)};
           constexpr uint32_t C = coef_bit(0, 0, 0, 2) | coef_bit(1, 0, 1, 1);
-          outer<1, 2, 2, C, MP>(A, LDF, tb, B, LDO, ta, w);
+          outer_tc<1, 2, 2, C, MP, true, false>(A, LDF, tb, B, LDO, ta, stg, w);
           put_cols(Yf, w[0]);
           put_cols(Yf + G::OWNC, w[1]);
         }
@@ -529,7 +684,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
           const uint32_t A[2] = {saddr(Pf), saddr(Qf)};
           const uint32_t B[2] = {saddr(Yf), saddr(Yf + G::OWNC)};
           constexpr uint32_t C = coef_bit(0, 0, 0, 1) | coef_bit(0, 1, 1, 1);
-          outer<2, 2, 1, C, MP>(A, LDF, tb, B, LDO, ta, z);
+          outer_tc<2, 2, 1, C, MP, true, false>(A, LDF, tb, B, LDO, ta, stg, z);
           put_cols(Zb, z[0]);
         }
         cl.sync();
@@ -610,12 +765,12 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
       const uint32_t A[1] = {saddr(Xf)};
       const uint32_t B[2] = {saddr(Ss), saddr(Ss + G::OWNC)};
       constexpr uint32_t C = coef_bit(0, 0, 0, 2) | coef_bit(1, 0, 1, 1);
-      outer<1, 2, 2, C, MP>(A, LDF, tb, B, LDO, ta, w);
+      outer_tc<1, 2, 2, C, MP, true, false>(A, LDF, tb, B, LDO, ta, stg, w);
       put_cols(Yf, w[0]);                           // d Sr  (this CTA's columns)
       put_cols(Yf + G::OWNC, w[1]);                 // d Si
     }
     float* Ub = Zb;                                 // [16][LDF] pivot-row panel of the inverse
-    float* Xb = Zb + 16 * LDF;                      // [16][MP] pivot columns, transposed
+    float* Xb = Zb + 16 * LDF;                      // [16][LDF] pivot columns, transposed
     float t = 1.0f;
     bool accepted = false;
     for (int bt = 0; bt < args.max_backtrack; ++bt) {
@@ -633,7 +788,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
         float k[1][4][4];
         const uint32_t A[1] = {saddr(Qf + r0)};
         const uint32_t B[1] = {saddr(Qf)};
-        outer<1, 1, 1, coef_bit(0, 0, 0, 2), MP>(A, LDF, ta, B, LDF, tb, k);
+        outer_tc<1, 1, 1, coef_bit(0, 0, 0, 2), MP, false>(A, LDF, ta, B, LDF, tb, stg, k);
 #pragma unroll
         for (int x = 0; x < 4; ++x)
 #pragma unroll
@@ -646,7 +801,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
       {
         const uint32_t A[1] = {saddr(Qf)};
         const uint32_t B[1] = {saddr(Yf + G::OWNC)};
-        outer<1, 1, 1, coef_bit(0, 0, 0, 2), MP>(A, LDF, tb, B, LDO, ta, u3);
+        outer_tc<1, 1, 1, coef_bit(0, 0, 0, 2), MP, true, false>(A, LDF, tb, B, LDO, ta, stg, u3);
       }
       cl.sync();                                    // K complete in both CTAs
       // Positive-definiteness test and inverse: Gauss-Jordan over 16-wide pivot blocks on the
@@ -714,7 +869,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
           }
           for (int e = tid; e < 16 * MP; e += THREADS) {
             const int i = e >> 4, q = e & 15;
-            Xb[q * MP + i] = Pf[i * LDF + kb + q];
+            Xb[q * LDF + i] = Pf[i * LDF + kb + q];
           }
         }
         __syncthreads();
@@ -735,7 +890,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
           if (!prow) {
 #pragma unroll 4
             for (int q = 0; q < 16; ++q) {
-              const float4 xv = ld4(Xb + q * MP + i0);
+              const float4 xv = ld4(Xb + q * LDF + i0);
               const float4 uv = ld4(Ub + q * LDF + jb);
 #pragma unroll
               for (int x = 0; x < 4; ++x)
@@ -754,7 +909,7 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
         {
           const uint32_t A[1] = {saddr(Pf)};
           const uint32_t B[1] = {saddr(Xf + r0)};
-          outer<1, 1, 1, coef_bit(0, 0, 0, 1), MP>(A, LDF, tb, B, LDF, ta, v);
+          outer_tc<1, 1, 1, coef_bit(0, 0, 0, 1), MP, true, false>(A, LDF, tb, B, LDF, ta, stg, v);
         }
         double tail[1] = {0.0};
 #pragma unroll

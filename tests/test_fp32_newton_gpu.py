@@ -94,7 +94,9 @@ def test_fp32_phase_agrees_with_all_fp64_newton(sp):
     a = sp.solve_ex(Td, precision="split")
     b = sp.solve_ex(Td, precision="split", fp32_newton=False)
     assert a.status.tolist() == b.status.tolist() == [0] * 8
-    assert rel_per_instance(a.X, b.X) < 1e-9 and rel_per_instance(a.omega, b.omega) < 1e-8
+    # both stop at a residual below feas_tol / 2 = 5e-9, so they agree to about that, and to
+    # the parity bound that holds each against the oracle
+    assert rel_per_instance(a.X, b.X) < XTOL and rel_per_instance(a.omega, b.omega) < XTOL
 
 
 def test_fp32_phase_with_the_adaptive_preconditioner(sp):
