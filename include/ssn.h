@@ -230,7 +230,8 @@ int ssn_cross_gram(const double* Ga, const double* Gd, int64_t g_stride, const d
  * workspace (workspace may be NULL).  SSN_PRECISION_SPLIT: INT8 Ozaki
  * products on the tcgen05 tensor cores (six balanced digits of every row of
  * [A D] and of [P Q], [-Q P], exact INT32 accumulation, FP64 recombination;
- * each entry within about 2^-45 K of its largest row contributions); needs
+ * each entry within about 2^-45 K of its largest row contributions; Ur and Ui
+ * 16-byte aligned); needs
  * ssn_recover_workspace_bytes of workspace.
  */
 size_t ssn_recover_workspace_bytes(int batch, int rows, int m);

@@ -351,6 +351,7 @@ int ssn_recover(const double* A, const double* D, int64_t ab_stride, const doubl
     return SSN_ERR_INVALID_ARGUMENT;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (split_form(opt)) {
+    if (!aligned16(Ur) || !aligned16(Ui)) return SSN_ERR_INVALID_ARGUMENT;   // 16-byte row-segment stores
     if (!workspace || workspace_bytes < ozaki_recover_workspace_bytes(batch, rows, m) || !aligned16(workspace))
       return SSN_ERR_WORKSPACE;
     return cuda_status(launch_recover_ozaki(A, D, ab_stride, P, Q, Ur, Ui, u_stride, batch, rows, m,

@@ -160,11 +160,18 @@ __device__ __forceinline__ void slice4(const double (&x)[4], double sc, uint32_t
   w[0] = __byte_perm(t4, t5, 0x7632) ^ 0x80808080u;   // byte 5 (most significant digit)
 }
 
+// An INT32 accumulator as a double, exactly: 2^52 + 2^31 + a has a + 2^31 as its low
+// word, so one XOR builds it and one subtraction removes the offset (an FP64 add
+// instead of an integer-to-FP64 conversion).
+__device__ __forceinline__ double i32_to_f64(uint32_t a) {
+  return __hiloint2double(0x43300000, static_cast<int>(a ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 // sum_l 256^(5-l) acc_l (Horner), the digit-level recombination before scaling.
 __device__ __forceinline__ double horner6(const uint32_t (&a)[kDigits]) {
-  double v = static_cast<double>(static_cast<int32_t>(a[0]));
+  double v = i32_to_f64(a[0]);
 #pragma unroll
-  for (int l = 1; l < kDigits; ++l) v = fma(v, 256.0, static_cast<double>(static_cast<int32_t>(a[l])));
+  for (int l = 1; l < kDigits; ++l) v = fma(v, 256.0, i32_to_f64(a[l]));
   return v;
 }
 
@@ -592,8 +599,8 @@ constexpr int kRBStep = oz::kDigits * kRW * kRK;          // 12288: stacked B di
 constexpr int kRStagesMax = 4;                            // digit-plane stages (bulk copies of W digits)
 constexpr int kRMmaWarp = 0;                              // warp 0: MMA issuer (lane 0), TMEM allocator
 constexpr int kRLoadWarp = 1;                             // warp 1: bulk copies of the W digit steps
-constexpr int kREpiWarp0 = 4;                             // warps 4-11: epilogue, TMEM lane quarter = warp % 4
-constexpr int kREpiWarps = 8;                             // two per lane quarter, one per 32-column half
+constexpr int kREpiWarp0 = 4;                             // warps 4-19: epilogue, TMEM lane quarter = warp % 4
+constexpr int kREpiWarps = 16;                            // four per lane quarter, one per 16-column quarter
 constexpr int kRThreads = (kREpiWarp0 + kREpiWarps) * 32;
 constexpr int kRSmemMax = 227 * 1024 - 1024;              // opt-in limit minus the static shared memory
 constexpr uint32_t kRSbo = (kRK / 16) * tc::kCoreBytes;    // 256
@@ -601,14 +608,14 @@ constexpr uint32_t kRTmemCols = 512;                      // 6 x 64 = 384 used
 
 __host__ __device__ inline int rec_groups(int m) { return cdiv(2 * m, kRW); }
 __host__ __device__ inline int rec_steps(int m) { return cdiv(2 * m, kRK); }
-constexpr int kREpiLd = 9;                                // padded row stride (doubles) of the epilogue transpose
-constexpr int kREpiBuf = 32 * kREpiLd * 8;                // 2304 bytes per epilogue warp
+constexpr int kRStgLd = kRW + 2;                          // staged X row stride (doubles): 528 bytes
+constexpr int kRStg = kRM * kRStgLd * 8;                  // 67584: one tile's X, staged for bulk stores
 __host__ __device__ inline int rec_stages(int m) {
-  const int f = (kRSmemMax - rec_steps(m) * kRBStep - kREpiWarps * kREpiBuf) / kRAStage;
+  const int f = (kRSmemMax - rec_steps(m) * kRBStep - kRStg) / kRAStage;
   return f > kRStagesMax ? kRStagesMax : f;
 }
 __host__ __device__ inline int rec_smem(int m) {
-  return rec_steps(m) * kRBStep + rec_stages(m) * kRAStage + kREpiWarps * kREpiBuf;
+  return rec_steps(m) * kRBStep + rec_stages(m) * kRAStage + kRStg;
 }
 
 // B row o, column c (o < 2m, c < 2m): rows [P_o | Q_o] (Ur), [-Q_o' | P_o'] (Ui).
@@ -758,7 +765,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
   const int32_t* rexp = row_exp + (size_t)b * rows;
   uint8_t* bsm = smem;                                              // nks x kRBStep
   uint8_t* asm_ = smem + nks * kRBStep;                             // nst x kRAStage
-  double* ebuf = reinterpret_cast<double*>(asm_ + nst * kRAStage);  // kREpiWarps x kREpiBuf bytes
+  double* stg = reinterpret_cast<double*>(asm_ + nst * kRAStage);   // kRM x kRStgLd: the tile's X
   const double nan = __longlong_as_double(0x7FF8000000000000ll);
 
   if (tid < kRW) {
@@ -825,19 +832,27 @@ __global__ void __launch_bounds__(kRThreads, 1)
       }
     }
   } else if (warp >= kREpiWarp0) {
-    // ---- epilogue warps: TMEM lane quarter (warp % 4), 32 of the 64 output columns, 32 rows
+    // ---- epilogue warps: TMEM lane quarter (warp % 4), 16 of the 64 output columns, 32 rows.
+    // Each lane recombines its row's levels into the staged tile; then one lane per row
+    // stores the row's segment of X (in Ur and/or Ui) with a bulk copy.
     const int ew = warp - kREpiWarp0, quarter = warp & 3;
-    const int c0 = (ew >> 2) * (kRW / 2);
-    double* buf = ebuf + ew * (kREpiBuf / 8);
+    const int c0 = (ew >> 2) * (kRW / 4);
     const uint32_t tbase = tc::tmem_at(tmem, quarter * 32, 0);
+    const int rr = quarter * 32 + lane;
+    double* srow = stg + rr * kRStgLd;
+    const int o0 = h * kRW, o1 = imin(o0 + kRW, 2 * m);
+    const int ur1 = imin(o1, m), ui0 = imax(o0, m);  // Ur columns [o0, ur1), Ui columns [ui0, o1) - m
+    const bool issuer = ew < 4;                         // one warp per lane quarter stores its rows
     for (int it = 0; it < ntl; ++it) {
       bool ok = tc::mbar_wait(&bar_acc_full, it & 1, tc::kWaitPolls) && !*reinterpret_cast<volatile int*>(&s_err);
       tc::fence_after_sync();
-      const int r0 = (tile0 + it) * kRM;
-      const int rr = quarter * 32 + lane, r = r0 + rr;
+      const int r = (tile0 + it) * kRM + rr;
       const int e = r < rows ? __ldg(rexp + r) : oz::kExpMin;
       const double rinv = e == oz::kExpNonFinite ? nan : oz::pow2(e - 26);
-      for (int jc = c0; jc < c0 + kRW / 2; jc += 8) {
+      if (issuer) tc::bulk_wait_read();                 // the previous tile's stores have read the staging
+      tc::named_sync(1, kREpiWarps * 32);
+#pragma unroll 1
+      for (int jc = c0; jc < c0 + kRW / 4; jc += 8) {
         uint32_t v[oz::kDigits][8];
         if (ok) {
 #pragma unroll
@@ -845,37 +860,37 @@ __global__ void __launch_bounds__(kRThreads, 1)
 #pragma unroll
           for (int l = 0; l < oz::kDigits; ++l) tc::tmem_wait8(v[l]);
         }
-        if (jc + 8 == c0 + kRW / 2) {               // all of this warp's TMEM reads of the tile are done
+        if (jc + 8 == c0 + kRW / 4) {               // all of this warp's TMEM reads of the tile are done
           tc::fence_before_sync();
           __syncwarp();
           if (lane == 0) tc::mbar_arrive(&bar_acc_free);
         }
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {
-          double corr = nan;
+        for (int jj = 0; jj < 8; jj += 2) {
+          double corr[2] = {nan, nan};
           if (ok) {
-            uint32_t a[oz::kDigits];
 #pragma unroll
-            for (int l = 0; l < oz::kDigits; ++l) a[l] = v[l][jj];
-            corr = oz::horner6(a) * rinv * s_finv[jc + jj];
-          }
-          buf[lane * kREpiLd + jj] = corr;
-        }
-        __syncwarp();
-        // transposed write-out: 4 rows x 8 columns (64-byte row segments) per instruction
+            for (int q = 0; q < 2; ++q) {
+              uint32_t a[oz::kDigits];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int lr = k * 4 + (lane >> 3), cc = lane & 7;
-          const int rw = r0 + quarter * 32 + lr, o = h * kRW + jc + cc;
-          if (rw < rows && o < 2 * m) {
-            const double cv = buf[lr * kREpiLd + cc];
-            if (o < m) Ur[(size_t)b * u_stride + (size_t)rw * m + o] = cv;
-            else Ui[(size_t)b * u_stride + (size_t)rw * m + (o - m)] = cv;
+              for (int l = 0; l < oz::kDigits; ++l) a[l] = v[l][jj + q];
+              corr[q] = oz::horner6(a) * rinv * s_finv[jc + jj + q];
+            }
           }
+          *reinterpret_cast<double2*>(srow + jc + jj) = make_double2(corr[0], corr[1]);
         }
-        __syncwarp();
+      }
+      tc::fence_smem_to_async();
+      tc::named_sync(1, kREpiWarps * 32);
+      if (issuer && r < rows) {
+        // m and o0 are even: every segment starts 16-byte aligned and has an even length
+        const size_t rowoff = (size_t)b * u_stride + (size_t)r * m;
+        if (o0 < ur1) tc::bulk_s2g(Ur + rowoff + o0, srow, (uint32_t)(ur1 - o0) * 8u);
+        if (ui0 < o1) tc::bulk_s2g(Ui + rowoff + (ui0 - m), srow + (ui0 - o0), (uint32_t)(o1 - ui0) * 8u);
+        tc::bulk_commit();
       }
     }
+    if (issuer) tc::bulk_wait_all();
   }
 
   tc::fence_before_sync();

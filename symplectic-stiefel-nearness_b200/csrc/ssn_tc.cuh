@@ -131,6 +131,24 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(mbar)) : "memory");
 }
 
+// Bulk (non-tensor) asynchronous copy of `bytes` contiguous bytes from this CTA's shared
+// memory to global memory, tracked in the issuing thread's bulk group.  dst, src 16-byte
+// aligned, bytes a multiple of 16.  The source must be made visible to the async proxy
+// (fence_smem_to_async by the writing threads, then a barrier) before the copy is issued.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+               :: "l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Wait until this thread's bulk groups have read their shared-memory sources.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Wait until this thread's bulk groups are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Barrier `id` (1..15) over `nthreads` threads (a multiple of 32) of the CTA.
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(nthreads) : "memory");
+}
+
 // TMEM address of (lane, column).
 __device__ __forceinline__ uint32_t tmem_at(uint32_t base, int lane, int col) {
   return base + (static_cast<uint32_t>(lane) << 16) + static_cast<uint32_t>(col);
