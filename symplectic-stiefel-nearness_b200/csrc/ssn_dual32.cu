@@ -105,61 +105,15 @@ __device__ __forceinline__ void st4(float* p, float a, float b, float c, float d
 }
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 
-// acc[o][x][y] = sum_k sum_(a,b) sign(o,a,b) A_a[k][4u + x] B_b[k][4v + y]: the 4 x 4 tile
-// (u, v) of sum op(A) op(B), with every operand given as K row segments (shared-memory
-// byte addresses, leading dims in floats).
-template <int NA, int NB, int NOUT, uint32_t COEF, int K>
-__device__ __forceinline__ void outer(const uint32_t (&A)[NA], int lda, int u, const uint32_t (&B)[NB], int ldb,
-                                      int v, float (&acc)[NOUT][4][4]) {
-#pragma unroll
-  for (int o = 0; o < NOUT; ++o)
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-      for (int y = 0; y < 4; ++y) acc[o][x][y] = 0.0f;
-  uint32_t pa[NA], pb[NB];
-#pragma unroll
-  for (int i = 0; i < NA; ++i) pa[i] = A[i] + 16u * u;
-#pragma unroll
-  for (int i = 0; i < NB; ++i) pb[i] = B[i] + 16u * v;
-  // operands of step k + 1 are loaded while step k's FFMAs run (the last step reloads row
-  // K - 1, which is in range and unused)
-  float4 an[NA], bn[NB];
-#pragma unroll
-  for (int i = 0; i < NA; ++i) an[i] = lds4(pa[i]);
-#pragma unroll
-  for (int i = 0; i < NB; ++i) bn[i] = lds4(pb[i]);
-#pragma unroll 2
-  for (int k = 0; k < K; ++k) {
-    float4 av[NA], bv[NB];
-#pragma unroll
-    for (int i = 0; i < NA; ++i) av[i] = an[i];
-#pragma unroll
-    for (int i = 0; i < NB; ++i) bv[i] = bn[i];
-    const uint32_t kn = static_cast<uint32_t>(k + 1 < K ? k + 1 : k);
-#pragma unroll
-    for (int i = 0; i < NA; ++i) an[i] = lds4(pa[i] + 4u * kn * lda);
-#pragma unroll
-    for (int i = 0; i < NB; ++i) bn[i] = lds4(pb[i] + 4u * kn * ldb);
-#pragma unroll
-    for (int o = 0; o < NOUT; ++o)
-#pragma unroll
-      for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib) {
-          const int sg = coef_get(COEF, o, ia, ib);
-          if (sg == 0) continue;
-#pragma unroll
-          for (int x = 0; x < 4; ++x) {
-            const float ax = sg == 2 ? -comp(av[ia], x) : comp(av[ia], x);
-#pragma unroll
-            for (int y = 0; y < 4; ++y) acc[o][x][y] = fmaf(ax, comp(bv[ib], y), acc[o][x][y]);
-          }
-        }
-  }
+// 1 / x from the hardware approximation and one Newton-Raphson step r (2 - x r), which
+// squares its relative error: the pivot reciprocal of the trial inverse, on its latency chain.
+__device__ __forceinline__ float rcp_nr(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;\n" : "=f"(r) : "f"(x));
+  return r * fmaf(-x, r, 2.0f);
 }
 
-// ---- the same products on the tensor cores: mma.sync m16n8k8 TF32 in the 3xTF32 form.
+// ---- products on the tensor cores: mma.sync m16n8k8 TF32 in the 3xTF32 form.
 // Each FP32 operand x is split as hi = tf32(x), lo = tf32(x - hi), and a product is
 // hi*hi + hi*lo + lo*hi with FP32 accumulation: about 2^-21 relative per product term
 // (the lo*lo term and the rounding of lo are below it), against 2^-24 for FFMA.
@@ -186,7 +140,9 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// outer() on the tensor cores, for the kernel's thread layout: lane l of a warp owns the
+// acc[o][x][y] = sum_k sum_(a,b) sign(o,a,b) A_a[k][4u + x] B_b[k][4v + y]: the 4 x 4 tile
+// (u, v) of sum op(A) op(B), with every operand given as K row segments (shared-memory
+// byte addresses, leading dims in floats), for the kernel's thread layout: lane l of a warp owns the
 // 4 x 4 tile (u, v) with u = u0 + (l >> 3), v = v0 + (l & 7) (TR = false: a 16 x 32 warp
 // tile, one m16 x four n8 MMA tiles) or u = u0 + (l & 7), v = v0 + (l >> 3) (TR = true:
 // 32 x 16, two m16 x two n8).  The accumulator fragments go through the warp's STAGE
@@ -827,15 +783,16 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
             float rowk[8];
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) rowk[jj] = __shfl_sync(0xffffffffu, rw[jj], kk + 16 * h);
-            ok = ok && (piv > 0.0f) && isfinite(piv);
-            const float inv = __frcp_rn(piv);
+            ok = ok & (piv > 0.0f) & (piv < INFINITY);
+            const float inv = rcp_nr(piv);
+            const float mik = aik * inv;            // the row multiplier: one rounding on the chain
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
               const bool colk = (h == hk) && (jj == ck);
               float v;
               if (i == kk) v = colk ? inv : rowk[jj] * inv;
-              else if (colk) v = -aik * inv;
-              else v = fmaf(-aik, rowk[jj] * inv, rw[jj]);
+              else if (colk) v = -mik;
+              else v = fmaf(-mik, rowk[jj], rw[jj]);
               rw[jj] = v;
             }
           }
@@ -867,9 +824,13 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
             }
             st4(Ub + p * LDF + j0, a0, a1, a2, a3);
           }
-          for (int e = tid; e < 16 * MP; e += THREADS) {
-            const int i = e >> 4, q = e & 15;
-            Xb[q * LDF + i] = Pf[i * LDF + kb + q];
+          for (int e = tid; e < 4 * MP; e += THREADS) {
+            const int i = e >> 2, c = e & 3;
+            const float4 xv = ld4(Pf + i * LDF + kb + 4 * c);
+            Xb[(4 * c + 0) * LDF + i] = xv.x;
+            Xb[(4 * c + 1) * LDF + i] = xv.y;
+            Xb[(4 * c + 2) * LDF + i] = xv.z;
+            Xb[(4 * c + 3) * LDF + i] = xv.w;
           }
         }
         __syncthreads();
