@@ -397,6 +397,39 @@ def run_ours(args):
         worst = {key: float(cert[key].max()) for key in ("feasibility", "stationarity", "delta")}
         Xs, Ws, Is = X.clone(), omega.clone(), iters.clone()
 
+        # the same solve with the library's built-in launch rules (autotune table cleared)
+        from symplectic_projection import autotune
+        table = autotune.installed()
+        cls = next((e for e in table if e["precision"] == precision and e["m"] == m
+                    and e["n_min"] <= n <= e["n_max"] and e["batch_min"] <= B <= e["batch_max"]), None)
+        builtin_ms = None
+        if cls is not None:
+            autotune.install([])
+            ub = lib.ssn_workspace_bytes(B, n, m)
+            uws = torch.empty(ub, dtype=torch.uint8, device=dev)
+
+            def builtin_call():
+                N.check(lib.ssn_solve(T.data_ptr(), X.data_ptr(), omega.data_ptr(), iters.data_ptr(),
+                                      status.data_ptr(), B, n, m, uws.data_ptr(), ub, N.ctypes.byref(opt), sh),
+                        "ssn_solve")
+            for _ in range(3):
+                builtin_call()
+            Ku = max(1, min(K, 50))
+            u0, u1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            u0.record(stream)
+            for _ in range(Ku):
+                builtin_call()
+            u1.record(stream)
+            torch.cuda.synchronize(dev)
+            builtin_ms = max_over_ranks(u0.elapsed_time(u1), dev) / Ku
+            autotune.install(table)
+            del uws
+        tuning = {"table_entries": len(table),
+                  "class_entry": {f: cls[f] for f in autotune.FIELDS} if cls else None,
+                  "tuned_ms_per_step": total_ms / K, "builtin_ms_per_step": builtin_ms,
+                  "note": "the autotune table's parameters for this class (0 = built-in rule) and the same "
+                          "solve timed with the built-in rules"}
+
         # phase breakdown (component entry points, no overlap between phases): Gram, eigh, recovery
         Kp = max(1, min(K, 30))
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(Kp)]
@@ -490,7 +523,8 @@ def run_ours(args):
         launches = (2 + 2 + 2 + (3 if fp32_on else 1) + 2) if split else 6
         return {"precision": precision, "ms_step": ms_step, "value": world * B / (ms_step * 1e-3),
                 "passed": passed, "worst": worst, "clocks": clocks, "per_launch": per_launch,
-                "phases": phases_out, "K": K, "X": Xs, "omega": Ws, "iters": Is, "launches": launches}
+                "phases": phases_out, "K": K, "X": Xs, "omega": Ws, "iters": Is, "launches": launches,
+                "autotune": tuning}
 
     forms = ["split", "fp64"] if args.precision == "both" else [args.precision]
     results = {f: timed_form(f) for f in forms}
@@ -541,7 +575,8 @@ def run_ours(args):
 
         rx, rw = relerr(head["X"], fp["X"]), relerr(head["omega"], fp["omega"])
         compare = {"fp64_form": {"value": fp["value"], "ms_per_step": fp["ms_step"], "all_pass": fp["passed"],
-                                 "worst": fp["worst"], "phases": fp["phases"], "clocks": fp["clocks"]},
+                                 "worst": fp["worst"], "phases": fp["phases"], "clocks": fp["clocks"],
+                                 "autotune": fp["autotune"]},
                    "split_over_fp64": head["value"] / fp["value"],
                    "split_vs_fp64_max_rel": {"X": float(rx.max()), "omega": float(rw.max()),
                                              "iterations_max_abs_diff":
@@ -604,7 +639,7 @@ def run_ours(args):
                     "pageable": {"value": world * B / (page_step * 1e-3), "unit": "solves/s",
                                  "ms_per_step": page_step, "input": "pageable host T"}},
             "gpu_launches": head["launches"] * K, "roofline": roofline, "solve_hbm": solve_hbm,
-            "peaks": dict(peaks), "phases": phases_out}
+            "peaks": dict(peaks), "phases": phases_out, "autotune": head["autotune"]}
     if compare:
         line.update(compare)
     if rank == 0 and world == 1 and not args.no_side_legs:

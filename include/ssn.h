@@ -104,6 +104,34 @@ enum {
   SSN_PRECOND_ADAPTIVE = 1
 };
 
+/*
+ * Launch parameters chosen by an autotuner for one problem class.  ssn_solve
+ * and ssn_solve_ragged (per shape group) look the table up by (precision, m,
+ * n, batch); the first matching entry wins, and a field of 0 keeps the
+ * library's built-in rule for that parameter.  No counterpart in the
+ * reference, which hard-codes its chunking and tiles (dual_recommended_hvp.py:13,
+ * gram_triangle_reflect.py:32-36).  The parameters change only the schedule:
+ * results agree with the built-in schedule's to the products' rounding.
+ */
+typedef struct {
+  int precision;      /* SSN_PRECISION_FP64 or SSN_PRECISION_SPLIT */
+  int m;              /* 2k */
+  int n_min, n_max;   /* inclusive range of n */
+  int batch_min, batch_max; /* inclusive range of the batch (or shape group) size */
+  int gram_splits;    /* FP64 Gram: row splits per instance, 1..64 */
+  int gram_chunks;    /* split-form Gram: row chunks per instance, 1..32 */
+  int recover_parts;  /* split-form recovery: parts of each (instance, column group)'s row tiles, 1..1024 */
+  int cluster;        /* Newton kernels: CTAs per instance, 1 or 2 (2 needs m > 32) */
+} ssn_tuning;
+
+/* Install `count` entries (copied; at most 1024; count 0 clears the table).
+ * Returns SSN_ERR_INVALID_ARGUMENT, leaving the table unchanged, if any entry
+ * is out of range.  Not to be called while another host thread is inside a
+ * solve.  ssn_get_tuning copies up to `capacity` entries out and returns how
+ * many are installed. */
+int ssn_set_tuning(const ssn_tuning* entries, int count);
+int ssn_get_tuning(ssn_tuning* entries, int capacity);
+
 /* Library version as 10000*major + 100*minor + patch. */
 int ssn_version(void);
 /* Static string naming a status code. */

@@ -45,8 +45,16 @@ SolveLayout solve_layout(int batch, int n, int m) {
   L.qfin = take(sizeof(double) * batch * mm);
   // the Gram partial sums share the Newton workspace (they are dead before it is used)
   const size_t work = sizeof(double) * (size_t)batch * kDualMats * mm;
-  size_t partial = sizeof(double) * gram_partial_doubles(batch, n, m);
-  const size_t oz = ozaki_gram_workspace_bytes(batch, n, m);
+  // each form's Gram plan under that form's tuning entry, as solve_batch will run it
+  size_t partial, oz;
+  {
+    TuningScope scope(find_tuning(SSN_PRECISION_FP64, n, m, batch));
+    partial = sizeof(double) * gram_partial_doubles(batch, n, m);
+  }
+  {
+    TuningScope scope(find_tuning(SSN_PRECISION_SPLIT, n, m, batch));
+    oz = ozaki_gram_workspace_bytes(batch, n, m);
+  }
   if (oz > partial) partial = oz;
   L.work = take(work > partial ? work : partial);
   L.eig_status = take(sizeof(int32_t) * batch);
@@ -183,6 +191,8 @@ bool solve_options_ok(const ssn_options* opt) { return options_ok(opt); }
 int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch,
                 int n, int m, void* workspace, const ssn_options* opt, cudaStream_t stream, int concurrent) {
   const SolveLayout L = solve_layout(batch, n, m);
+  // the problem class's autotuned launch parameters, for every launch below
+  TuningScope tuning(find_tuning(split_form(opt) ? SSN_PRECISION_SPLIT : SSN_PRECISION_FP64, n, m, batch));
   char* ws = static_cast<char*>(workspace);
   double* Cr = reinterpret_cast<double*>(ws + L.cr);
   double* Ci = reinterpret_cast<double*>(ws + L.ci);

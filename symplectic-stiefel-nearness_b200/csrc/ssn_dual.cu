@@ -941,7 +941,11 @@ static cudaError_t launch_dual_mb(const DualArgs& args, int batch, cudaStream_t 
 
 // Two CTAs per instance when the batch leaves half the SMs idle and m is large
 // enough for the row split to pay; one otherwise.
-int dual_cluster_size(int batch, int m) { return (m >= 48 && 2 * batch <= sm_count()) ? 2 : 1; }
+int dual_cluster_size(int batch, int m) {
+  const ssn_tuning* tune = active_tuning();
+  if (tune && tune->cluster > 0) return (tune->cluster == 2 && m > 32) ? 2 : 1;   // autotuned
+  return (m >= 48 && 2 * batch <= sm_count()) ? 2 : 1;
+}
 
 static cudaError_t launch_dual_phase(const DualArgs& args, int batch, bool two, cudaStream_t stream) {
   switch (bucket_of(args.m)) {

@@ -46,6 +46,8 @@ struct GramSplit {
 static GramSplit gram_split(int batch, int rows, int max_splits = 1 << 30) {
   const int sms = device_sm_count();
   int want = imin(cdiv(2 * sms, batch), 16);
+  const ssn_tuning* tune = active_tuning();
+  if (tune && tune->gram_splits > 0) want = tune->gram_splits;   // autotuned
   want = imax(1, imin(imin(want, cdiv(rows, 64)), max_splits));
   int chunk = round_up(cdiv(rows, want), kPanelK);
   int splits = cdiv(rows, chunk);

@@ -17,6 +17,20 @@ constexpr int kDualMats = 23;
 // the query fails).  Safe to call from several host threads.
 int current_device_sm_count();
 
+// The autotuned launch parameters that apply to the launches the calling host thread
+// is enqueueing (set by ssn_solve for its problem class), or null: the built-in rules.
+const ssn_tuning* active_tuning();
+// The first installed entry matching (precision, n, m, batch), or null.
+const ssn_tuning* find_tuning(int precision, int n, int m, int batch);
+// Makes `t` the calling thread's active tuning for the scope's lifetime.
+struct TuningScope {
+  const ssn_tuning* prev;
+  explicit TuningScope(const ssn_tuning* t);
+  ~TuningScope();
+  TuningScope(const TuningScope&) = delete;
+  TuningScope& operator=(const TuningScope&) = delete;
+};
+
 struct DualArgs {
   int m;
   int max_newton, max_cg, max_backtrack;

@@ -533,6 +533,9 @@ OzGramPlan oz_gram_plan(int batch, int rows, int m) {
       best = nc;
     }
   }
+  const ssn_tuning* tune = active_tuning();
+  if (tune && tune->gram_chunks > 0 && round_up(cdiv(rows, tune->gram_chunks), kScaleRows) <= max_chunk)
+    best = tune->gram_chunks;                     // autotuned
   const int chunk = round_up(cdiv(rows, best), kScaleRows);
   return OzGramPlan{chunk, cdiv(rows, chunk), ncg};
 }
@@ -959,7 +962,9 @@ cudaError_t launch_recover_products(const double* P, const double* Q, double* Ur
   if (err != cudaSuccess) return err;
   // tiles of an (instance, group) split into parts: about four CTAs per SM over the grid
   const int ntiles = cdiv(rows, kRM), pairs = batch * rec_groups(m);
-  const int nparts = imax(1, imin(ntiles, cdiv(4 * sm_count_oz(), pairs)));
+  const ssn_tuning* tune = active_tuning();
+  const int want = (tune && tune->recover_parts > 0) ? tune->recover_parts : cdiv(4 * sm_count_oz(), pairs);
+  const int nparts = imax(1, imin(ntiles, want));
   ozaki_recover_kernel<<<dim3(nparts * rec_groups(m), batch), kRThreads, smem, stream>>>(
       w.wdig, w.row_exp, w.bdig, w.fexp, Ur, Ui, u_stride, rows, m, nparts, w.stall);
   return cudaGetLastError();

@@ -57,6 +57,8 @@ PROTOTYPES = {
     "ssn_inverse_from_cholesky": (_I, [_P, _P, _I, _I, _P]),
     "ssn_spd_inverse": (_I, [_P, _P, _P, _I, _I, _P]),
     "ssn_cholesky_k": (_I, [_P, _P, _P, _I, _I, _P]),
+    "ssn_set_tuning": (_I, [_P, _I]),
+    "ssn_get_tuning": (_I, [_P, _I]),
 }
 
 SSN_OK = 0
@@ -71,6 +73,14 @@ class Options(ctypes.Structure):
                 ("precision", ctypes.c_int), ("eig_sweeps", ctypes.c_int),
                 ("preconditioner", ctypes.c_int), ("fp32_newton", ctypes.c_int),
                 ("reserved", ctypes.c_int * 4)]
+
+
+class Tuning(ctypes.Structure):
+    """ssn_tuning (include/ssn.h): launch parameters for one problem class; 0 = built-in rule."""
+    _fields_ = [("precision", ctypes.c_int), ("m", ctypes.c_int), ("n_min", ctypes.c_int),
+                ("n_max", ctypes.c_int), ("batch_min", ctypes.c_int), ("batch_max", ctypes.c_int),
+                ("gram_splits", ctypes.c_int), ("gram_chunks", ctypes.c_int),
+                ("recover_parts", ctypes.c_int), ("cluster", ctypes.c_int)]
 
 
 # ssn_options.precision / .preconditioner values (include/ssn.h)
@@ -95,6 +105,8 @@ def load() -> ctypes.CDLL:
             fn.restype = res
             fn.argtypes = args
         _lib = lib
+        from . import autotune
+        autotune.load()        # the committed per-(n, k) table, when present
     return _lib
 
 

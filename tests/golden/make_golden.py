@@ -1,9 +1,12 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
-Run in a container that has the reference checked out (read-only) at
-``/root/reference`` (override with SSN_REFERENCE_ROOT):
+Run with a checkout of the reference project (read-only) available:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--reference PATH]
+
+The reference root is, in order: ``--reference PATH``, the environment
+variable SSN_REFERENCE_ROOT, or ``reference`` beside this repository's root
+directory (``<repo>/../reference``).  It must contain ``src/symplectic_projection``.
 
 What it does:
   * installs a stub ``cupy`` module (the reference imports CuPy at module
@@ -33,7 +36,20 @@ import numpy as np
 import torch
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("SSN_REFERENCE_ROOT", "/root/reference"))
+REPO = HERE.parents[1]
+
+
+def reference_root(argv=None) -> Path:
+    """--reference PATH, else $SSN_REFERENCE_ROOT, else <repo>/../reference."""
+    import argparse
+    p = argparse.ArgumentParser(description="generate the golden fixtures from the reference")
+    p.add_argument("--reference", default=None, help="root of the reference project checkout")
+    args, _ = p.parse_known_args(argv)
+    root = args.reference or os.environ.get("SSN_REFERENCE_ROOT") or str(REPO.parent / "reference")
+    return Path(root).resolve()
+
+
+REF = reference_root([] if __name__ != "__main__" else None)
 
 # (name, n, k, batch, case_index, target transform)
 CASES = [
