@@ -42,9 +42,10 @@ PRECISION_NOTE = {
 }
 N_DEFAULT, K_DEFAULT, BATCH_DEFAULT = 4096, 48, 64
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per target at n = 4096, k = 48 from
-# single-kernel ncu captures of 16 targets (each target's state is private, so traffic scales with
-# the number of targets).
-DRAM_BYTES_PER_TARGET_C2 = {"newton_fp32": (3644672 + 0) / 16}
+# single-kernel ncu captures of 24 targets (each target's state is private, so traffic scales with
+# the number of targets): dual32_kernel 5.42 MB read, 0 written; the FP64 tail of dual_kernel
+# 9.32 MB read, 0.71 MB written.
+DRAM_BYTES_PER_TARGET_C2 = {"newton_fp32": (5423360 + 0) / 24, "newton_fp64": (9324032 + 709120) / 24}
 HBM_FALLBACK_GBS = 6650.0        # copy bandwidth of this GPU type when no measured figure is present
 
 
@@ -547,8 +548,10 @@ def run_ours(args):
         achieved = fl / (ms * 1e-3) / 1e12
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["fp32"], "unit": "TFLOP/s",
                     "frac": achieved / peaks["fp32"], "traffic": traffic, "kernel": "dual32_kernel (FP32 Newton)",
-                    "peak_source": "FP32 SGEMM rate (TF32 off) measured in this run through cuBLAS; the "
-                                   "kernel runs FP32 FFMA products, no tensor cores"}
+                    "peak_source": "FP32 SGEMM rate (TF32 off) measured in this run through cuBLAS, the "
+                                   "FP32-accurate library rate; the kernel runs its products as TF32 mma.sync "
+                                   "(3xTF32 where they set the iterate, one TF32 product in the HVPs and the "
+                                   "line search's change), counted here as FP32 product flops"}
     else:
         achieved = (fl / (ms * 1e-3) / 1e12) if fl else None
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -924,7 +927,10 @@ def run_illcond(args):
             "data": "synthetic: T = U diag(s) V^T, U, V from QR of seeded Gaussians, s log-uniform in [1e-2, 1e2]",
             "config": {"workload": f"{B} x ({2 * n} x {m}) ill-conditioned FP64 targets, n={n}, k={k}, "
                                    f"{8 * B * 2 * n * m / 1e9:.1f} GB of T",
-                       "precision": PRECISION_NOTE[precision] + "; adaptive CG preconditioner; adjoint FP64",
+                       "precision": PRECISION_NOTE[precision] + "; adaptive CG preconditioner; adjoint FP64"
+                                    + ("; at m = 128 the FP32 Newton phase does not apply (its state fits on "
+                                       "chip up to m = 96), so every Newton step is FP64"
+                                       if precision == "split" and 2 * k > 96 else ""),
                        "inputs": "T and G resident in HBM", "parallelism": "replicas x1",
                        "generation_s": gen_s},
             "forward_ms": fwd_ms, "backward_ms": bwd_ms,
