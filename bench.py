@@ -647,6 +647,11 @@ def run_ours(args):
         line.update(compare)
     if rank == 0 and world == 1 and not args.no_side_legs:
         line["reference_gpu"] = reference_gpu(args)
+        # the ragged workload (config 3) in the same run, so the default line carries it
+        rg = run_ragged(args, emit=False)
+        line["ragged"] = {key: rg[key] for key in ("metric", "value", "unit", "ms_per_step", "all_pass", "worst",
+                                                   "e2e", "gpu_launches")}
+        line["ragged"]["workload"] = rg["config"]["workload"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, args.cpu_seconds)
         line["cpu_baseline_1thread"] = cpu_baseline(args, min(args.cpu_seconds, 8.0), threads=1)
@@ -658,8 +663,9 @@ def run_ours(args):
 
 
 
-def run_ragged(args):
-    """The ragged workload: 384 targets, n in {512 .. 8192}, k in {8 .. 64}, one ssn_solve_ragged call per step."""
+def run_ragged(args, emit=True):
+    """The ragged workload: 384 targets, n in {512 .. 8192}, k in {8 .. 64}, one ssn_solve_ragged call per step.
+    Prints its JSON line (emit) or returns it."""
     import torch
     import symplectic_projection as sp
     from symplectic_projection import _native as N
@@ -752,6 +758,8 @@ def run_ragged(args):
             "e2e": {"value": count / (e2e_ms * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": 8 * tt,
                     "d2h_bytes_per_step": 8 * (tt + ww) + count * 12, "ms_per_step": e2e_ms},
             "gpu_launches": launches * K}
+    if not emit:
+        return line
     print(json.dumps(line))
     return 0 if passed else 1
 

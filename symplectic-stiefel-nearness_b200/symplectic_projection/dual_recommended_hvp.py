@@ -11,6 +11,7 @@ batch on a Newton or line-search cap, as the reference does
 """
 from __future__ import annotations
 
+import os
 import threading
 from dataclasses import dataclass
 
@@ -129,10 +130,25 @@ def solve_ragged(targets, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
         ms.append(m)
     dev = torch.device("cuda", torch.cuda.current_device()) if on_host else targets[0].device
     if on_host:
-        # one pinned staging buffer: the copy up runs at the link's pinned rate
+        with _host_lock:
+            return _solve_ragged_call(targets, ns, ms, dev, True, max_newton, max_cg, max_backtrack, feas_tol,
+                                      precision, eig_sweeps, preconditioner, fp32_newton, raise_on_failure)
+    return _solve_ragged_call(targets, ns, ms, dev, False, max_newton, max_cg, max_backtrack, feas_tol,
+                              precision, eig_sweeps, preconditioner, fp32_newton, raise_on_failure)
+
+
+def _solve_ragged_call(targets, ns, ms, dev, on_host, max_newton, max_cg, max_backtrack, feas_tol, precision,
+                       eig_sweeps, preconditioner, fp32_newton, raise_on_failure):
+    if on_host:
+        # pack into the package's cached pinned staging buffer (no per-call pinned
+        # allocation), with the per-target copies spread over host threads; the copy up
+        # then runs at the link's pinned rate
         total = sum(t.numel() for t in targets)
-        staged = torch.empty(total, dtype=torch.float64, pin_memory=True)
-        torch.cat([t.reshape(-1) for t in targets], out=staged)
+        staged = _staging_buffer(dev, _RAGGED_SLOT, (total,))
+        offs = [0]
+        for t in targets:
+            offs.append(offs[-1] + t.numel())
+        _parallel_copies([(staged[offs[i]:offs[i + 1]], t.reshape(-1)) for i, t in enumerate(targets)])
         flat = staged.to(dev, non_blocking=True)
     else:
         flat = torch.cat([t.reshape(-1) for t in targets])
@@ -162,13 +178,46 @@ def solve_ragged(targets, *, max_newton: int = MAX_NEWTON, max_cg: int = MAX_CG,
     if raise_on_failure:
         raise_for_status(status)
     if on_host:
-        X_host = torch.empty(X.shape, dtype=X.dtype, pin_memory=True)
-        X_host.copy_(X, non_blocking=True)
+        # X comes back through the (now free) pinned staging buffer at the link's pinned rate,
+        # then into one fresh host tensor per target, the caller's to keep
+        staged_x = _staging_buffer(dev, _RAGGED_SLOT, (X.numel(),))
+        staged_x.copy_(X, non_blocking=True)
         omega, iterations, status = omega.cpu(), iterations.cpu(), status.cpu()   # synchronises
-        X = X_host
-    Xs = [X[t_off[i]:t_off[i] + 2 * ns[i] * ms[i]].view(2 * ns[i], ms[i]) for i in range(count)]
+        Xs = [torch.empty(2 * ns[i], ms[i], dtype=torch.float64) for i in range(count)]
+        _parallel_copies([(Xs[i].view(-1), staged_x[t_off[i]:t_off[i] + 2 * ns[i] * ms[i]]) for i in range(count)])
+    else:
+        Xs = [X[t_off[i]:t_off[i] + 2 * ns[i] * ms[i]].view(2 * ns[i], ms[i]) for i in range(count)]
     Ws = [omega[w_off[i]:w_off[i] + ms[i] * ms[i]].view(ms[i], ms[i]) for i in range(count)]
     return Xs, Ws, iterations, status
+
+
+_copy_pool = None
+
+
+def _parallel_copies(pairs) -> None:
+    """dst.copy_(src) for host tensor pairs, spread over a pool of host threads (torch
+    releases the GIL in copy_), in chunks of about equal bytes."""
+    global _copy_pool
+    if _copy_pool is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _copy_pool = ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
+    workers = _copy_pool._max_workers
+    total = sum(d.numel() for d, _ in pairs)
+    chunks, cur, size = [], [], 0
+    for d, src in pairs:
+        cur.append((d, src))
+        size += d.numel()
+        if size * workers >= total and len(chunks) < workers - 1:
+            chunks.append(cur)
+            cur, size = [], 0
+    if cur:
+        chunks.append(cur)
+
+    def run(chunk):
+        for d, src in chunk:
+            d.copy_(src)
+    for f in [_copy_pool.submit(run, c) for c in chunks]:
+        f.result()
 
 
 def raise_for_status(status: torch.Tensor) -> None:
@@ -235,6 +284,9 @@ def _stream_pool(dev: torch.device):
     if key not in _streams:
         _streams[key] = [torch.cuda.Stream(dev) for _ in range(N_STREAMS)]
     return _streams[key]
+
+
+_RAGGED_SLOT = 1 << 20          # staging slot of the ragged host path (the chunked path uses 0 ..)
 
 
 def _staging_buffer(dev: torch.device, slot: int, shape) -> torch.Tensor:

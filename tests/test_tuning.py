@@ -70,3 +70,19 @@ def test_committed_table_is_valid(at):
     for e in entries:
         assert any(e[f] for f in at.FIELDS)
         assert e["tuned_ms"] <= e["builtin_ms"]
+
+
+def test_parallel_host_copies():
+    import torch
+    from symplectic_projection.dual_recommended_hvp import _parallel_copies
+    g = torch.Generator().manual_seed(5)
+    srcs = [torch.randn(int(n), dtype=torch.float64, generator=g) for n in torch.randint(1, 5000, (97,), generator=g)]
+    flat = torch.empty(sum(s.numel() for s in srcs), dtype=torch.float64)
+    offs = [0]
+    for s in srcs:
+        offs.append(offs[-1] + s.numel())
+    _parallel_copies([(flat[offs[i]:offs[i + 1]], s) for i, s in enumerate(srcs)])
+    assert torch.equal(flat, torch.cat(srcs))
+    outs = [torch.empty_like(s) for s in srcs]
+    _parallel_copies([(o, flat[offs[i]:offs[i + 1]]) for i, o in enumerate(outs)])
+    assert all(torch.equal(o, s) for o, s in zip(outs, srcs))
