@@ -786,14 +786,15 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
             ok = ok & (piv > 0.0f) & (piv < INFINITY);
             const float inv = rcp_nr(piv);
             const float mik = aik * inv;            // the row multiplier: one rounding on the chain
+            const bool prow = i == kk;               // the pivot row is scaled, the others eliminated
+            const float a = prow ? 0.0f : -mik;
+            const float sc = prow ? inv : 1.0f;
+            const float pc = prow ? inv : -mik;      // the new pivot column entry
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
               const bool colk = (h == hk) && (jj == ck);
-              float v;
-              if (i == kk) v = colk ? inv : rowk[jj] * inv;
-              else if (colk) v = -mik;
-              else v = fmaf(-mik, rowk[jj], rw[jj]);
-              rw[jj] = v;
+              const float v = fmaf(a, rowk[jj], rw[jj] * sc);   // prow: rowk * inv; else rw - mik rowk
+              rw[jj] = colk ? pc : v;
             }
           }
 #pragma unroll
