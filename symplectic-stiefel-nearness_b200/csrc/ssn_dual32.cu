@@ -8,8 +8,10 @@
 //     gradient and residual, PCG with HVPs, the trial's positive-definiteness
 //     test and inverse, Armijo with the exact objective change -- while the
 //     FP32 residual is at least switch_tol (1e-5; FP32 resolves the residual
-//     of these problems to about 1e-7).  It writes omega in FP64 and the
-//     number of Newton updates it took;
+//     of these problems to about 1e-7) and still improving (three steps
+//     without a new best, or half the Newton cap, hand over: ill-conditioned
+//     targets can have an FP32 residual floor above switch_tol).  It writes
+//     omega in FP64 and the number of Newton updates it took;
 //  3. dual_kernel warm-started from that omega: P = (I + omega^2)^-1 in FP64
 //     with the positive-definiteness test, then the last Newton step(s) with
 //     FP64 sandwich, residual, trial inverse and line search, and convergence
@@ -454,6 +456,8 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
   int iterations = 0, n_step = 0, n_hvp = 0, n_trial = 0, n_fallback = 0;
   const double sqrt_m = sqrt((double)m);
   const bool go = status_in == SSN_INSTANCE_CONVERGED;
+  double best_res = INFINITY;      // the FP32 residual's best so far, and steps since it
+  int since_best = 0;
 
   for (int step = 0; go && step < args.max_newton; ++step) {
     ++n_step;
@@ -592,6 +596,16 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
     const double gnorm = sqrt(gn2);
     const double residual = gnorm * s / sqrt_m;
     if (!(residual >= args.switch_tol)) break;      // converged far enough for FP32, or non-finite
+    // stalled: on ill-conditioned targets the FP32 residual can have a floor above switch_tol;
+    // three steps without a new best residual, or half the Newton cap spent, hand over to the
+    // FP64 iteration (both CTAs hold the same FP64 sums, so they leave together)
+    if (residual < best_res) {
+      best_res = residual;
+      since_best = 0;
+    } else if (++since_best >= 3) {
+      break;
+    }
+    if (2 * step >= args.max_newton) break;
     ++iterations;
 
     // ---- search direction (:137-164); g, r, d, p are exactly antisymmetric, den symmetric

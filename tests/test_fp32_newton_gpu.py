@@ -111,6 +111,20 @@ def test_fp32_phase_with_the_adaptive_preconditioner(sp):
     assert st.tolist() == [0, 0] and bool((cnt[:, 4] >= 1).all())
 
 
+@pytest.mark.parametrize("n,k", [(512, 48), (300, 40)])
+def test_fp32_phase_with_the_adaptive_preconditioner_on_a_cluster(sp, n, k):
+    # m = 96 and m = 80 run the FP32 phase on a 2-CTA cluster with the adaptive denominators
+    from symplectic_projection.inputs import illcond_targets
+    T = illcond_targets(n, k, 2)
+    Xo, Wo, Io = O.solve(T, preconditioner="adaptive")
+    X, W, it = sp.solve(T, precision="split", preconditioner="adaptive")
+    assert rel_per_instance(X, Xo) < XTOL and rel_per_instance(W, Wo) < XTOL
+    for rec in O.inspect_output(T, X):
+        assert O.passes(rec), rec
+    cnt, st, _ = newton_counters(T, preconditioner="adaptive")
+    assert st.tolist() == [0, 0] and bool((cnt[:, 4] >= 1).all())
+
+
 def test_fp32_phase_isolates_a_nonfinite_instance(sp):
     T, _ = O.make_inputs(256, 32, 2, 3)
     T[1, 5, 3] = float("nan")
