@@ -60,8 +60,10 @@ def newton_counters(T, precision="split", **opts):
     return counters.cpu(), status.cpu(), iters.cpu()
 
 
-# (n, k, batch): m = 24 (one CTA, 32-padded), 32, 64 (a cluster), 80 (a cluster, 96-padded), 96
-SHAPES = [(96, 12, 4), (2048, 16, 8), (256, 32, 6), (300, 40, 3), (4096, 48, 4)]
+# (n, k, batch): m = 24 (one CTA, 32-padded), 32, 64 (a cluster), 80 (a cluster, 96-padded), 96,
+# and a single target (the golden fixtures' square and near-square targets run the split form in
+# the split-form parity tests)
+SHAPES = [(96, 12, 4), (2048, 16, 8), (256, 32, 6), (300, 40, 3), (4096, 48, 4), (4096, 48, 1)]
 
 
 @pytest.mark.parametrize("n,k,B", SHAPES)
