@@ -385,6 +385,13 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
     Pf[e] = (i == j) ? 1.0f : 0.0f;
     Qf[e] = 0.0f;
   }
+  // stall bookkeeping of the FP32 residual (best so far, steps since), double-buffered by step
+  __shared__ float s_best[2];
+  __shared__ int s_since[2];
+  if (tid == 0) {
+    s_best[0] = INFINITY;
+    s_since[0] = 0;
+  }
   __threadfence();
   cl.sync();
 
@@ -456,8 +463,6 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
   int iterations = 0, n_step = 0, n_hvp = 0, n_trial = 0, n_fallback = 0;
   const double sqrt_m = sqrt((double)m);
   const bool go = status_in == SSN_INSTANCE_CONVERGED;
-  double best_res = INFINITY;      // the FP32 residual's best so far, and steps since it
-  int since_best = 0;
 
   for (int step = 0; go && step < args.max_newton; ++step) {
     ++n_step;
@@ -598,14 +603,19 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
     if (!(residual >= args.switch_tol)) break;      // converged far enough for FP32, or non-finite
     // stalled: on ill-conditioned targets the FP32 residual can have a floor above switch_tol;
     // three steps without a new best residual, or half the Newton cap spent, hand over to the
-    // FP64 iteration (both CTAs hold the same FP64 sums, so they leave together)
-    if (residual < best_res) {
-      best_res = residual;
-      since_best = 0;
-    } else if (++since_best >= 3) {
-      break;
+    // FP64 iteration.  Every thread reads the same bookkeeping (slot step & 1, written by
+    // thread 0 one step earlier, many barriers ago) and both CTAs hold the same FP64 sums,
+    // so all leave together.
+    {
+      const int par = step & 1;
+      const bool better = (float)residual < s_best[par];
+      const int since = better ? 0 : s_since[par] + 1;
+      if (threadIdx.x == 0) {
+        s_best[par ^ 1] = better ? (float)residual : s_best[par];
+        s_since[par ^ 1] = since;
+      }
+      if (since >= 3 || 2 * step >= args.max_newton) break;
     }
-    if (2 * step >= args.max_newton) break;
     ++iterations;
 
     // ---- search direction (:137-164); g, r, d, p are exactly antisymmetric, den symmetric
@@ -800,15 +810,14 @@ __global__ void __launch_bounds__(G32<MB, CL>::THREADS, 1) dual32_kernel(Dual32A
             ok = ok & (piv > 0.0f) & (piv < INFINITY);
             const float inv = rcp_nr(piv);
             const float mik = aik * inv;            // the row multiplier: one rounding on the chain
-            const bool prow = i == kk;               // the pivot row is scaled, the others eliminated
-            const float a = prow ? 0.0f : -mik;
-            const float sc = prow ? inv : 1.0f;
-            const float pc = prow ? inv : -mik;      // the new pivot column entry
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
               const bool colk = (h == hk) && (jj == ck);
-              const float v = fmaf(a, rowk[jj], rw[jj] * sc);   // prow: rowk * inv; else rw - mik rowk
-              rw[jj] = colk ? pc : v;
+              float v;
+              if (i == kk) v = colk ? inv : rowk[jj] * inv;
+              else if (colk) v = -mik;
+              else v = fmaf(-mik, rowk[jj], rw[jj]);
+              rw[jj] = v;
             }
           }
 #pragma unroll
