@@ -164,7 +164,7 @@ __device__ __forceinline__ void outer_tc(const uint32_t (&A)[NA], int lda, int u
     for (int q = 0; q < MT * NT; ++q)
 #pragma unroll
       for (int e = 0; e < 4; ++e) c[o][q][e] = 0.0f;
-#pragma unroll 1
+#pragma unroll 2
   for (int k = 0; k < K; k += 8) {
 #pragma unroll
     for (int mi = 0; mi < MT; ++mi) {
