@@ -192,6 +192,7 @@ def _solve_ragged_call(targets, ns, ms, dev, on_host, max_newton, max_cg, max_ba
 
 
 _copy_pool = None
+_COPY_WORKERS = min(16, os.cpu_count() or 1)
 
 
 def _parallel_copies(pairs) -> None:
@@ -200,8 +201,8 @@ def _parallel_copies(pairs) -> None:
     global _copy_pool
     if _copy_pool is None:
         from concurrent.futures import ThreadPoolExecutor
-        _copy_pool = ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
-    workers = _copy_pool._max_workers
+        _copy_pool = ThreadPoolExecutor(max_workers=_COPY_WORKERS)
+    workers = _COPY_WORKERS
     total = sum(d.numel() for d, _ in pairs)
     chunks, cur, size = [], [], 0
     for d, src in pairs:
