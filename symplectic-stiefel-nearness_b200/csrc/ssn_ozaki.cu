@@ -330,6 +330,12 @@ __global__ void __launch_bounds__(kGThreads, 1)
   const int nsub = cdiv(r1 - r0, kGSub);
   const int mp16 = round_up(m, 16);
   const GramSmem L = gram_smem(m);
+  // slicing warps that work: the fewest of 8, 12, 16 that take the sub-tile's tasks (16 columns
+  // x 2 row octets each) in as few rounds as 16 would, so every working warp has as many tasks
+  // (m = 96: 24 tasks, 12 warps x 2 rather than 16 warps x 1 or 2)
+  const int ntask_all = (mp16 / 16) * 4;
+  const int rounds16 = cdiv(ntask_all, kGSliceWarps);
+  const int nsl = cdiv(ntask_all, 8) == rounds16 ? 8 : cdiv(ntask_all, 12) == rounds16 ? 12 : kGSliceWarps;
   const double* Ab = A + (size_t)b * ab_stride;
   const double* Db = D + (size_t)b * ab_stride;
   uint8_t* dbase = smem;
@@ -350,10 +356,10 @@ __global__ void __launch_bounds__(kGThreads, 1)
   if (tid == 0) {
     for (int s = 0; s < kGFStagesMax; ++s) {
       tc::mbar_init(&bar_full[s], 1);
-      tc::mbar_init(&bar_ffree[s], kGSliceWarps);
+      tc::mbar_init(&bar_ffree[s], nsl);
     }
     for (int s = 0; s < kGDStages; ++s) {
-      tc::mbar_init(&bar_ready[s], kGSliceWarps);
+      tc::mbar_init(&bar_ready[s], nsl);
       tc::mbar_init(&bar_dfree[s], 1);
     }
     s_err = 0;
@@ -405,7 +411,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         }
         if (!ok) atomicExch(&s_err, 1);
       }
-    } else {
+    } else if (warp < nsl) {
       // ---- slicing warps: every sub-tile, FP64 stage -> digit planes and the stacked B copy
       const int ntask = (mp16 / 16) * 4;                  // warp tasks: 16 columns x 2 row octets
       for (int t = 0; t < nsub; ++t) {
@@ -419,7 +425,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         uint8_t* stage = dbase + d * L.dstage;
         const double* fs = reinterpret_cast<const double*>(fbase + f * L.fstage);
         const int nr = imin(kGSub, r1 - (r0 + t * kGSub));
-        for (int g = warp; g < ntask; g += kGSliceWarps) {
+        for (int g = warp; g < ntask; g += nsl) {
           // lane -> (column, K octet) so that every half-warp reads 16 distinct columns of a
           // staged row (conflict-free 8-byte loads) and writes 16 distinct bank pairs of the
           // digit planes (conflict-free 8-byte stores): lanes 8-15 take the upper 8 columns
