@@ -136,25 +136,19 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   // thread takes the same decision)
   int sweeps_cap = max_sweeps;
   if (skip_corr > 0.0f) {
-    double mx = 0.0;
+    // c_pq^2 >= skip^2 c_pp c_qq for some pair (no square root or division per entry)
+    const double s2 = static_cast<double>(skip_corr) * static_cast<double>(skip_corr);
+    int keep = 0;
     for (int e = tid; e < m * m; e += kJacobiThreads) {
       const int i = e / m, j = e - i * m;
       if (i < j) {
         const double d = C[(size_t)i * m + i] * C[(size_t)j * m + j];
         const double c = fabs(C[e]);
-        if (d > 0.0) mx = fmax(mx, c / sqrt(d));
-        else if (c > 0.0 || !(d == 0.0)) mx = fmax(mx, 1.0);   // non-finite or inconsistent: keep the sweeps
+        if (d > 0.0) keep |= (c * c >= s2 * d) ? 1 : 0;
+        else if (c > 0.0 || !(d == 0.0)) keep = 1;   // non-finite or inconsistent: keep the sweeps
       }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    __syncthreads();
-    if ((tid & 31) == 0) red[tid >> 5] = mx;
-    __syncthreads();
-    double all = 0.0;
-    for (int w = 0; w < kJacobiThreads / 32; ++w) all = fmax(all, red[w]);
-    if (!(all >= static_cast<double>(skip_corr))) sweeps_cap = 0;
-    __syncthreads();
+    if (!__syncthreads_or(keep)) sweeps_cap = 0;
   }
   // block list: off-diagonal blocks (a < b) row-major, then the diagonal blocks.
   // Host blocks carry kHostFlag in .y and are skipped by the generic threads.
