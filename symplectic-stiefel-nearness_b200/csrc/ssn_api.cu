@@ -101,29 +101,36 @@ constexpr int kDefaultEigSweeps = 1;
 // the sandwich carries the off-diagonal part.  Ill-conditioned Grams keep the sweep.
 constexpr float kRoughBasisSkip = 0.1f;
 
-// A side stream forked from the caller's stream with events (and joined back the
-// same way), so work that only depends on the inputs can overlap later kernels.
-// The stream and its two events are created once per host thread and device and
-// kept: nothing is created or destroyed inside a call, so a call can be captured
-// into a CUDA graph (the fork and join become graph edges).  Calls from one
-// thread share the stream; the events order each call's side work correctly.
+// The split form's two streams.  The recovery's W digits depend only on T, so a
+// side stream of the LOWEST priority makes them while the Newton kernels run, and
+// the solve itself runs on a stream of the HIGHER priority: the block scheduler
+// hands freed SMs to pending CTAs of the higher-priority stream first, so the
+// digit kernel's 4096 short CTAs fill what the Newton kernels leave over instead
+// of delaying them.  (At equal priority they delayed the eigen and Newton launches
+// by about 0.23 ms at 64 x 8192 x 96, nearly the digit kernel's whole run.)
+// Streams and events are created once per host thread and kept, and every fork and
+// join is an event, so a call can be captured into a CUDA graph (they become edges).
+constexpr int kMaxDevices = 64;
+
+// The side stream of the calling thread on the current device.  Calls from one
+// thread share it; the events order each call's side work correctly.
 struct SideStream {
   cudaStream_t stream = nullptr;
-  cudaEvent_t forked = nullptr, done = nullptr;
-  cudaError_t fork(cudaStream_t parent) {
+  cudaEvent_t forked = nullptr, done = nullptr;   // `forked`: recorded by launch_dual
+  cudaError_t open() {
     struct Pool {
       cudaStream_t stream = nullptr;
       cudaEvent_t forked = nullptr, done = nullptr;
     };
-    constexpr int kMaxDevices = 64;
     thread_local Pool pool[kMaxDevices];
-    int dev = 0;
+    int dev = 0, least = 0, greatest = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     Pool& p = pool[dev];
     if (!p.stream) {
-      e = cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking);
+      e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+      if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&p.stream, cudaStreamNonBlocking, least);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.forked, cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming);
       if (e != cudaSuccess) return e;
@@ -131,12 +138,68 @@ struct SideStream {
     stream = p.stream;
     forked = p.forked;
     done = p.done;
-    e = cudaEventRecord(forked, parent);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, forked, 0);
-    return e;
+    return cudaSuccess;
   }
+  cudaError_t wait_forked() { return cudaStreamWaitEvent(stream, forked, 0); }
   cudaError_t record() { return cudaEventRecord(done, stream); }
   cudaError_t join(cudaStream_t parent) { return cudaStreamWaitEvent(parent, done, 0); }
+};
+
+// The stream the split solve runs on: the caller's own when its priority is above
+// the lowest, else a highest-priority stream forked from it (one per caller stream,
+// thread and device, up to kMainSlots of them; past that the caller's stream).
+struct MainStream {
+  static constexpr int kMainSlots = 32;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  cudaError_t fork(cudaStream_t parent) {
+    struct Slot {
+      int dev = -1;
+      cudaStream_t parent = nullptr, stream = nullptr;
+      cudaEvent_t forked = nullptr, done = nullptr;
+    };
+    thread_local Slot slots[kMainSlots];
+    stream = parent;
+    done = nullptr;
+    int dev = 0, least = 0, greatest = 0, pr = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamGetPriority(parent, &pr);
+    if (e != cudaSuccess) return e;
+    if (greatest >= least || pr < least) return cudaSuccess;
+    Slot* s = nullptr;
+    for (Slot& c : slots) {
+      if (c.dev == dev && c.parent == parent) {
+        s = &c;
+        break;
+      }
+      if (!s && c.dev < 0) s = &c;
+    }
+    if (!s) return cudaSuccess;                  // every slot taken: stay on the caller's stream
+    if (s->dev < 0) {
+      // no stream is created while the caller's stream is being captured
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if ((e = cudaStreamIsCapturing(parent, &cs)) != cudaSuccess) return e;
+      if (cs != cudaStreamCaptureStatusNone) return cudaSuccess;
+      e = cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, greatest);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->forked, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+      s->dev = dev;
+      s->parent = parent;
+    }
+    e = cudaEventRecord(s->forked, parent);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->stream, s->forked, 0);
+    if (e != cudaSuccess) return e;
+    stream = s->stream;
+    done = s->done;
+    return cudaSuccess;
+  }
+  cudaError_t join(cudaStream_t parent) {
+    if (!done) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(done, stream);
+    return e == cudaSuccess ? cudaStreamWaitEvent(parent, done, 0) : e;
+  }
 };
 
 void fill_options(const ssn_options* opt, DualArgs& a) {
@@ -180,16 +243,9 @@ cudaError_t eigenbasis(const ssn_options* opt, const double* Cr, double* values,
   return launch_eigh(Cr, values, vectors, scale, sweeps, status, batch, m, ws, stream);
 }
 
-}  // namespace
-
-namespace ssn {
-
-size_t solve_workspace_bytes(int batch, int n, int m) { return solve_layout(batch, n, m).total; }
-bool solve_options_ok(const ssn_options* opt) { return options_ok(opt); }
-
-// Arguments checked by the caller (ssn_solve, ssn_solve_ragged).
-int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch,
-                int n, int m, void* workspace, const ssn_options* opt, cudaStream_t stream, int concurrent) {
+// The solve pipeline on one stream (the split form's side work on the side stream).
+int solve_on(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch, int n,
+             int m, void* workspace, const ssn_options* opt, cudaStream_t stream, int concurrent) {
   const SolveLayout L = solve_layout(batch, n, m);
   // the problem class's autotuned launch parameters, for every launch below
   TuningScope tuning(find_tuning(split_form(opt) ? SSN_PRECISION_SPLIT : SSN_PRECISION_FP64, n, m, batch));
@@ -212,15 +268,8 @@ int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, 
   cudaError_t e = split ? launch_gram_ozaki(A, D, stride, Cr, Ci, batch, n, m, work, nullptr, stall, stream)
                         : launch_gram(A, D, stride, Cr, Ci, batch, n, m, work, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
-  // split form: the digits of [A | D] for the recovery do not depend on the dual solution, so
-  // they are made on a side stream while the (latency-bound) eigen and Newton kernels run
   SideStream side;
-  if (split) {
-    e = side.fork(stream);
-    if (e == cudaSuccess) e = launch_recover_wdigits(A, D, stride, batch, n, m, ws + L.rec, side.stream);
-    if (e == cudaSuccess) e = side.record();
-    if (e != cudaSuccess) return SSN_ERR_CUDA;
-  }
+  if (split && side.open() != cudaSuccess) return SSN_ERR_CUDA;
   int32_t* sweeps = reinterpret_cast<int32_t*>(ws + L.sweeps);
   e = eigenbasis(opt, Cr, values, vectors, scale, sweeps, eig_status, batch, m, ws + L.eig_ws, stream);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
@@ -242,16 +291,41 @@ int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, 
   a.status = status;
   a.counters = nullptr;
   a.concurrent = concurrent;
-  e = launch_dual(a, batch, stream);
+  e = launch_dual(a, batch, stream, split ? side.forked : nullptr);
   if (e != cudaSuccess) return SSN_ERR_CUDA;
   if (split) {
-    e = side.join(stream);
+    // the digits of [A | D] for the recovery do not depend on the dual solution: made on
+    // the side stream from the start of the Newton steps (side.forked), beside them
+    e = side.wait_forked();
+    if (e == cudaSuccess) e = launch_recover_wdigits(A, D, stride, batch, n, m, ws + L.rec, side.stream);
+    if (e == cudaSuccess) e = side.record();
+    if (e == cudaSuccess) e = side.join(stream);
     if (e == cudaSuccess)
       e = launch_recover_products(Pf, Qf, X, X + (size_t)n * m, stride, batch, n, m, ws + L.rec, stream);
   } else {
     e = launch_recover(A, D, stride, Pf, Qf, X, X + (size_t)n * m, stride, batch, n, m, stream);
   }
   return cuda_status(e);
+}
+
+}  // namespace
+
+namespace ssn {
+
+size_t solve_workspace_bytes(int batch, int n, int m) { return solve_layout(batch, n, m).total; }
+bool solve_options_ok(const ssn_options* opt) { return options_ok(opt); }
+
+// Arguments checked by the caller (ssn_solve, ssn_solve_ragged).  The split form runs
+// on a higher-priority stream than its side work (MainStream), joined back into `stream`
+// also after an error, so nothing enqueued here outlives the caller's view of it.
+int solve_batch(const double* T, double* X, double* omega, int64_t* iterations, int32_t* status, int batch,
+                int n, int m, void* workspace, const ssn_options* opt, cudaStream_t stream, int concurrent) {
+  if (!split_form(opt)) return solve_on(T, X, omega, iterations, status, batch, n, m, workspace, opt, stream, concurrent);
+  MainStream main;
+  if (main.fork(stream) != cudaSuccess) return SSN_ERR_CUDA;
+  const int rc = solve_on(T, X, omega, iterations, status, batch, n, m, workspace, opt, main.stream, concurrent);
+  const cudaError_t e = main.join(stream);
+  return rc != SSN_OK ? rc : cuda_status(e);
 }
 
 }  // namespace ssn

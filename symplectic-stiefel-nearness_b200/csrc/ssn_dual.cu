@@ -976,7 +976,7 @@ static cudaError_t mark(int i, cudaStream_t stream) {
   return t_newton_events_set ? cudaEventRecord(t_newton_events[i], stream) : cudaSuccess;
 }
 
-cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
+cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream, cudaEvent_t side_fork) {
   const int cl = dual_cluster_size(imax(batch, args.concurrent), args.m);
   const bool two = cl == 2;
   cudaError_t e = mark(0, stream);
@@ -985,6 +985,7 @@ cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
     DualArgs a = args;
     a.phase = 0;
     if ((e = mark(1, stream)) != cudaSuccess || (e = mark(2, stream)) != cudaSuccess) return e;
+    if (side_fork && (e = cudaEventRecord(side_fork, stream)) != cudaSuccess) return e;
     e = launch_dual_phase(a, batch, two, stream);
     return e == cudaSuccess ? mark(3, stream) : e;
   }
@@ -993,6 +994,7 @@ cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream) {
   a.phase = 1;
   e = launch_dual_phase(a, batch, two, stream);
   if (e == cudaSuccess) e = mark(1, stream);
+  if (e == cudaSuccess && side_fork) e = cudaEventRecord(side_fork, stream);
   if (e != cudaSuccess) return e;
   Dual32Args b{};
   b.m = args.m;

@@ -130,7 +130,9 @@ cudaError_t launch_eigh(const double* Cr, double* values, double* vectors, doubl
 cudaError_t launch_eigh_approx(const double* Cr, double* values, double* vectors, double* scale,
                                int32_t* sweeps, int32_t* status, int batch, int m, void* workspace,
                                int max_sweeps, bool fp32, float skip_corr, cudaStream_t stream);
-cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream);
+// side_fork (may be null) is recorded on the stream where the Newton steps start (before
+// the FP32 phase, else before the FP64 iteration): work that waits on it overlaps them.
+cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream, cudaEvent_t side_fork = nullptr);
 // Measurement hook behind ssn_set_newton_events (per host thread; null clears).
 void set_newton_events(void* const* events);
 // The whole uniform-batch solve (the body of ssn_solve) on one stream; `concurrent` as in DualArgs.

@@ -176,15 +176,17 @@ int ssn_solve_ragged(const double* T, double* X, double* omega, int64_t* iterati
   const int64_t* t_off_d = reinterpret_cast<const int64_t*>(ws + plan.t_off_at);
   const int64_t* w_off_d = reinterpret_cast<const int64_t*>(ws + plan.w_off_at);
 
-  // fork: one side stream per group, up to kRaggedStreams, all after the plan upload
+  // fork: one side stream per group, up to kRaggedStreams, all after the plan upload; at
+  // the highest priority, so the split form's digit kernels (lowest) only fill idle SMs
   const int ns = imin(kRaggedStreams, (int)plan.groups.size());
   cudaStream_t side[kRaggedStreams] = {};
   cudaEvent_t forked = nullptr, joined[kRaggedStreams] = {};
-  int rc = SSN_OK;
-  e = cudaEventCreateWithFlags(&forked, cudaEventDisableTiming);
+  int rc = SSN_OK, least = 0, greatest = 0;
+  e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&forked, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventRecord(forked, stream);
   for (int s = 0; s < ns && e == cudaSuccess; ++s) {
-    e = cudaStreamCreateWithFlags(&side[s], cudaStreamNonBlocking);
+    e = cudaStreamCreateWithPriority(&side[s], cudaStreamNonBlocking, greatest);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&joined[s], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(side[s], forked, 0);
   }
