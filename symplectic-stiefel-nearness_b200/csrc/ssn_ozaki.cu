@@ -718,8 +718,10 @@ __global__ void __launch_bounds__(256)
       const int c = c0 + 2 * i;                       // m even: a pair never straddles A and D
       double2 v = make_double2(0.0, 0.0);
       if (r < rows && c < 2 * m)
-        v = c < m ? __ldg(reinterpret_cast<const double2*>(Ab + (size_t)r * m + c))
-                  : __ldg(reinterpret_cast<const double2*>(Db + (size_t)r * m + (c - m)));
+        // streaming (evict-first) loads and stores: this kernel runs beside the Newton
+        // kernels, whose operands it would otherwise push out of L2
+        v = c < m ? __ldcs(reinterpret_cast<const double2*>(Ab + (size_t)r * m + c))
+                  : __ldcs(reinterpret_cast<const double2*>(Db + (size_t)r * m + (c - m)));
       x[2 * i] = v.x;
       x[2 * i + 1] = v.y;
     }
@@ -741,7 +743,7 @@ __global__ void __launch_bounds__(256)
     const int s = c0 / kRK, k = c0 - s * kRK;
     uint8_t* blk = out + (size_t)s * kRAStage + tc::core_offset(rr, k, kRK);
 #pragma unroll
-    for (int q = 0; q < oz::kDigits; ++q) *reinterpret_cast<uint2*>(blk + q * kRPlane) = make_uint2(w0[q], w1[q]);
+    for (int q = 0; q < oz::kDigits; ++q) __stcs(reinterpret_cast<uint2*>(blk + q * kRPlane), make_uint2(w0[q], w1[q]));
   }
 }
 
