@@ -516,7 +516,8 @@ def run_ours(args):
         phases_out["hbm_floor_ms"] = 48.0 * n * m * B / (hbm_gbs * 1e9) * 1e3
         phases_out["note"] = ("gram, eigh and recover timed one after another through the component entry "
                               "points; the newton_* launches timed inside ssn_solve by the library's event hook "
-                              "(the full solve overlaps the split form's recovery digits with eigh and Newton)")
+                              "(the full solve makes the split form's recovery digits on a lowest-priority side "
+                              "stream beside the Newton kernels; recover here includes them)")
         ms_step = total_ms / K
         # kernels per solve: split = scale, Ozaki Gram, finalize, recovery digits, 2 Jacobi, Newton
         # (set-up, FP32, FP64 or one), recovery prep and products; FP64 = Gram, finalize, 2 Jacobi,
