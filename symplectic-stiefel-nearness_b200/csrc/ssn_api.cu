@@ -105,9 +105,9 @@ constexpr float kRoughBasisSkip = 0.1f;
 // side stream of the LOWEST priority makes them while the Newton kernels run, and
 // the solve itself runs on a stream of the HIGHER priority: the block scheduler
 // hands freed SMs to pending CTAs of the higher-priority stream first, so the
-// digit kernel's 4096 short CTAs fill what the Newton kernels leave over instead
-// of delaying them.  (At equal priority they delayed the eigen and Newton launches
-// by about 0.23 ms at 64 x 8192 x 96, nearly the digit kernel's whole run.)
+// digit kernel's short CTAs (2048 at 64 x 8192 x 96) fill what the Newton kernels
+// leave over instead of delaying them.  (At equal priority they delayed the eigen
+// and Newton launches by about 0.23 ms there, nearly the digit kernel's whole run.)
 // Streams and events are created once per host thread and kept, and every fork and
 // join is an event, so a call can be captured into a CUDA graph (they become edges).
 constexpr int kMaxDevices = 64;
