@@ -977,7 +977,15 @@ static cudaError_t mark(int i, cudaStream_t stream) {
 }
 
 cudaError_t launch_dual(const DualArgs& args, int batch, cudaStream_t stream, cudaEvent_t side_fork) {
-  const int cl = dual_cluster_size(imax(batch, args.concurrent), args.m);
+  int cl = dual_cluster_size(imax(batch, args.concurrent), args.m);
+  // The split form's FP32 phase holds m in (64, 96] on a 2-CTA cluster only.  Unless the
+  // autotune table fixes the cluster, take it there even where the rule above gives one
+  // CTA (more instances than half the SMs, as in large or ragged batches): a few FP32
+  // steps and one FP64 step on two SMs cost less SM time than every step in FP64 on one.
+  const ssn_tuning* tune = active_tuning();
+  if (args.fp32_newton && args.approx_basis && !(tune && tune->cluster > 0) && !dual32_supported(args.m, cl) &&
+      dual32_supported(args.m, 2))
+    cl = 2;
   const bool two = cl == 2;
   cudaError_t e = mark(0, stream);
   if (e != cudaSuccess) return e;

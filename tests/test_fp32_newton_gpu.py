@@ -90,6 +90,22 @@ def test_fp32_phase_runs_and_hands_over(sp, n, k, B):
     assert int((it - it64).abs().max()) <= 1
 
 
+def test_fp32_phase_runs_for_more_instances_than_half_the_sms(sp):
+    # m = 96 with 80 instances: the default cluster rule gives one CTA per instance there,
+    # where the FP32 phase cannot hold its state; the split form takes the 2-CTA cluster
+    # instead, so the FP32 phase still runs
+    B = 80
+    T, _ = O.make_inputs(128, 48, 3, B)
+    cnt, st, _ = newton_counters(T)
+    assert st.tolist() == [0] * B
+    assert bool((cnt[:, 4] >= 2).all())
+    X, W, it = sp.solve(T, precision="split")
+    Xo, Wo, Io = O.solve(T[:4])
+    assert rel_per_instance(X[:4], Xo) < XTOL and rel_per_instance(W[:4], Wo) < XTOL
+    for rec in O.inspect_output(T, X):
+        assert O.passes(rec), rec
+
+
 def test_fp32_phase_agrees_with_all_fp64_newton(sp):
     T, _ = O.make_inputs(4096, 48, 5, 8)
     Td = T.cuda()
