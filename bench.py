@@ -31,6 +31,10 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "symplectic-stiefel-nearness_b200"))
+# More hardware work queues than CUDA's default 8 (read when the context is created): the
+# end-to-end leg keeps 16 caller streams in flight, each forking the solve's own streams,
+# and the ragged call one stream per shape group (16 with these queues).
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "solves/s, 64×(8192×96) batch, all pass r_F/r_G/δ checks: split-prec vs FP64"
 PRECISION_NOTE = {
